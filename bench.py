@@ -1,0 +1,410 @@
+"""Benchmark: track-layer updates/s of the propagate-to-z + Kalman-update hot
+path on B200 (one JSON line on rank 0).
+
+Workload (one GPU): 1000 events x 9600 tracks, 20 layers, FP32, bsize-32
+AOSOA -- the physics workload (charge +-1, pT log-uniform 0.5-20 GeV, phi
+uniform, eta 1.6-2.5, vertex z ~ N(0, 5 cm), correlated PD covariances, hits on
+20 planes z = 30..270 cm at the true helix point plus 30 um / 1 um noise),
+generated from a fixed seed.  A step is one pass of the hot path over all 9.6M
+tracks x 20 layers.  Inputs (8.1 GB) are larger than L2, so no flush is needed.
+
+  value   device-resident throughput (p2z_run_device, CUDA events on the stream)
+  e2e     the same metric through p2z_run from pinned host buffers, host->device
+          and device->host copies inside the timed region
+  batched_vs_plain  uneven events (2000 events, log-normal track counts,
+          5-20 hits per track with 10% of layers dropped): the persistent
+          work-queue kernel replayed as a CUDA graph vs one launch per event
+
+`--impl reference` times the reference's own CPU hot loop (its OpenMP source
+compiled unchanged into oracle/_ref) on this host's cores, on the same
+workload, one bounded sample of events per step.
+
+Multi-GPU (torchrun): every rank runs its own 1000 events (weak scaling, no
+data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+
+# Algorithmic work per track-layer update (reduced form, z row zero):
+#   FP32 flops (FMA = 2): propagation scalars 30 + Jacobian 55 + J C J^T 142
+#   + 2-D Kalman update 122 = 349.
+#   Compulsory bytes: 6 hit words (24 B) + track in and out (2 x 112 B) over
+#   20 layers (11.2 B) = 35.2 B.
+FLOPS_PER_UPDATE = 349
+BYTES_PER_UPDATE = 35.2
+FP32_LANES_PER_SM = 128
+
+METRIC = "track-layer updates/s on 1 B200, batched vs plain, <=1e-5 rel err vs FP64"
+WORKLOAD = "physics 1000 events x 9600 tracks x 20 layers, bsize 32, FP32 (precise form)"
+
+
+def load_p2z():
+    pkg = ROOT / "p2z-tests_b200"
+    spec = importlib.util.spec_from_file_location("p2z_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["p2z_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic_per_update():
+    """dram bytes per update from the committed ncu summary of the kernel, if any."""
+    p = ROOT / "profiles" / "k_flat_v2_physics.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_update:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier_max(world, value):
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def uneven_counts(n_events, seed):
+    rng = np.random.default_rng(seed)
+    c = np.exp(np.log(3000.0) + 1.0 * rng.standard_normal(n_events))
+    return np.clip(np.rint(c), 50, 30000).astype(np.int64)
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    p2z = load_p2z()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    if not O.ref_available("b32"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference tree)"}))
+        return 0
+    cores = os.cpu_count() or 1
+    n_ev = args.ref_events
+    cfg = p2z.make_config(bsize=32, nevts=n_ev, ntrks=9600, nlayer=20)
+    trk, hit = p2z.generate_physics(cfg)
+    upd = n_ev * 9600 * 20
+    for _ in range(args.warmup):
+        O.ref_run(trk, hit, nev=n_ev, nthreads=cores)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.ref_run(trk, hit, nev=n_ev, nthreads=cores)
+        ts.append(time.perf_counter() - t0)
+    sec = float(np.sum(ts))
+    value = upd * args.steps / sec
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_events_per_step": n_ev, "host_threads": cores},
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"{n_ev} events x 9600 tracks x 20 layers per step, OpenMP over events"},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(p2z, trk, hit):
+    """The reference's hot loop on this host's cores, on a bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    if not O.ref_available("b32"):
+        return None
+    cores = os.cpu_count() or 1
+    n_ev = 50
+    nb = n_ev * 300
+    t, h = np.ascontiguousarray(trk[:nb]), np.ascontiguousarray(hit[:nb])
+    O.ref_run(t, h, nev=n_ev, nthreads=cores)
+    reps, sec = 0, 0.0
+    while sec < 10.0 and reps < 200:
+        t0 = time.perf_counter()
+        O.ref_run(t, h, nev=n_ev, nthreads=cores)
+        sec += time.perf_counter() - t0
+        reps += 1
+    return {"value": n_ev * 9600 * 20 * reps / sec, "unit": "updates/s", "cores": cores, "kind": "reference",
+            "sample": f"{n_ev} of the 1000 events, {reps} passes ({sec:.1f} s wall), reference OMP build, "
+                      f"{cores} threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-events", type=int, default=50)
+    ap.add_argument("--nevts", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    p2z = load_p2z()
+    ctx = p2z.Context(local)
+    stream = torch.cuda.current_stream()
+
+    nev = args.nevts
+    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat")
+    params = p2z.physics_params(seed=20240601 + rank)
+    trk, hit = p2z.generate_physics(cfg, params)
+    updates = nev * 9600 * 20
+    dt = torch.from_numpy(trk).cuda()
+    dh = torch.from_numpy(hit).cuda()
+    do = torch.empty_like(dt)
+
+    def step(c=cfg):
+        rc = p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), dt.data_ptr(), dh.data_ptr(), None, do.data_ptr(),
+                                    p2z.C.c_void_p(stream.cuda_stream), None)
+        if rc != p2z.OK:
+            raise p2z.P2zError(rc, p2z.lib.p2z_last_error(ctx.h).decode())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier(world)
+    ms_max = barrier_max(world, ms)
+    ms_step = ms_max / args.steps
+    value = updates * world / (ms_step / 1e3)
+    st = ctx.run_device(cfg, dt, dh, do)  # one more pass for the launch count and status
+    launches_per_step = st.launches
+
+    # e2e: host buffers through p2z_run
+    e2e = None
+    if not args.no_e2e:
+        pin_t = p2z.PinnedArray(trk.shape)
+        pin_h = p2z.PinnedArray(hit.shape)
+        pin_o = p2z.PinnedArray(trk.shape)
+        pin_t.array[...] = trk
+        pin_h.array[...] = hit
+        del dt, dh, do
+        torch.cuda.empty_cache()
+        ecfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat")
+        for _ in range(3):
+            ctx.run(ecfg, pin_t.array, pin_h.array, pin_o.array)
+        barrier(world)
+        tot = 0.0
+        n_e2e = max(3, min(args.steps, 10))
+        for _ in range(n_e2e):
+            s = ctx.run(ecfg, pin_t.array, pin_h.array, pin_o.array)
+            tot += s.total_ms
+        tot = barrier_max(world, tot)
+        e2e = {"value": updates * world / (tot / n_e2e / 1e3), "unit": "updates/s",
+               "h2d_bytes_per_step": int(s.h2d_bytes), "d2h_bytes_per_step": int(s.d2h_bytes),
+               "ms_per_step": tot / n_e2e, "steps": n_e2e,
+               "path": "p2z_run, pinned host buffers, 8 chunks on 2 streams (copy/compute overlap)"}
+        out_ok = bool(np.isfinite(pin_o.array[:, :6, :]).all())
+        pin_t.free(); pin_h.free(); pin_o.free()
+    else:
+        del dt, dh, do
+        out_ok = None
+    torch.cuda.empty_cache()
+
+    # batched (persistent + graph) vs plain (one launch per event) on uneven events
+    bvp = None
+    if not args.no_uneven:
+        counts = uneven_counts(2000, 77 + rank)
+        ucfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20)
+        ut, uh, um = p2z.generate_physics(ucfg, p2z.physics_params(seed=99 + rank), with_mask=True)
+        p2z.mask_layers(um, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=5 + rank)
+        u_upd = int(np.unpackbits(um.view(np.uint8)).sum())
+        udt, udh = torch.from_numpy(ut).cuda(), torch.from_numpy(uh).cuda()
+        udo = torch.empty_like(udt)
+        udm = torch.from_numpy(um.view(np.int32)).cuda()
+        res = {}
+        for sched in ("persistent", "per_event"):
+            c = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=sched)
+            for _ in range(3):
+                p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), udt.data_ptr(), udh.data_ptr(), udm.data_ptr(),
+                                       udo.data_ptr(), p2z.C.c_void_p(stream.cuda_stream), None)
+            torch.cuda.synchronize()
+            barrier(world)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            n = max(3, args.steps // 2)
+            a.record(stream)
+            for _ in range(n):
+                p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), udt.data_ptr(), udh.data_ptr(), udm.data_ptr(),
+                                       udo.data_ptr(), p2z.C.c_void_p(stream.cuda_stream), None)
+            b.record(stream)
+            torch.cuda.synchronize()
+            t_ms = barrier_max(world, a.elapsed_time(b)) / n
+            res[sched] = u_upd * world / (t_ms / 1e3)
+        bvp = {"workload": "2000 events, track counts log-normal (median 3000, sigma 1, clipped 50-30000), "
+                           "5-20 hits/track, 10% layers dropped",
+               "tracks": int(counts.sum()), "updates_per_step": u_upd,
+               "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
+               "ratio": res["persistent"] / res["per_event"]}
+        del udt, udh, udo, udm
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    peaks = measured_peaks()
+    launch_ms = ms_step / max(1, launches_per_step)
+    achieved_gbs = BYTES_PER_UPDATE * updates / launches_per_step / (launch_ms / 1e3) / 1e9
+    tpu = profile_traffic_per_update()
+    sm_max = clk["sm_max_mhz"] or 1965.0
+    fp32_peak = 148 * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
+    fp32_ach = FLOPS_PER_UPDATE * updates / (launch_ms / 1e3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
+                   "updates_per_step_per_gpu": updates, "l2": "inputs 8.1 GB > L2, no flush",
+                   "parallelism": f"dp{world} (independent event shards)"},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved_gbs / peaks["hbm_gbs"],
+                     "traffic": (tpu * updates / launches_per_step) if tpu else None,
+                     "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                     "bytes_per_update": BYTES_PER_UPDATE},
+        "fp32_roofline": {"achieved": fp32_ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": fp32_ach / fp32_peak,
+                          "flops_per_update": FLOPS_PER_UPDATE,
+                          "peak_source": f"148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (nominal, no measured "
+                                         f"FP32 peak on this pool)"},
+        "clocks": clk,
+        "gpu_launches": launches_per_step * args.steps,
+        "e2e": e2e,
+        "batched_vs_plain": bvp,
+        "outputs_finite": out_ok,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p2z, trk, hit)
+    print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

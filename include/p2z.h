@@ -1,0 +1,289 @@
+/*
+ * p2z.h -- C ABI of the B200 propagate-to-z + Kalman-update library (libp2z.so).
+ *
+ * The reference benchmark has no library boundary: its "API" is a set of C++
+ * free functions compiled into each executable together with main().  This
+ * header is the thin extern "C" layer that replaces them.  Every entry point
+ * names the reference interface it stands in for (file:line inside the
+ * reference project).  Signatures use plain pointers, sizes and enums only.
+ *
+ * Data layout (unchanged from the reference, src/propagate-toz-test_OMP.cpp:57-125):
+ *   A track batch (MPTRK) of width B holds element p of track t at data[t + p*B]:
+ *     float par[6*B]   x, y, z, ipt (= 1/pT), phi, theta
+ *     float cov[21*B]  packed lower triangle of the symmetric 6x6 covariance,
+ *                      (i,j) with i >= j at i*(i+1)/2 + j   (SymOffsets66, :52-55)
+ *     int   q[B]       charge
+ *   sizeof(MPTRK) = 28*B*4 bytes.
+ *   A hit batch (MPHIT) of width B:
+ *     float pos[3*B]   x, y, z
+ *     float cov[6*B]   packed lower triangle of the 3x3 hit covariance
+ *   sizeof(MPHIT) = 9*B*4 bytes.
+ *   Track batches of event e are consecutive (bTk: batch ib of event e at ib + nb*e,
+ *   :147-153).  The hits of track batch b on layer l are hit batch l + nlayer*b
+ *   (bHit, :215-217), i.e. the layers of a batch are contiguous.
+ *
+ * Uneven events (no counterpart in the reference, which fixes ntrks per event):
+ *   event e holds ceil(n_e/B) batches; the batches of all events are consecutive
+ *   and the last batch of an event may be partly filled.  A per-track-slot hit
+ *   mask (one uint32 per slot, slot = batch*B + t, bit l = "track has a hit on
+ *   layer l") marks missing layers; a layer whose bit is clear is skipped
+ *   entirely (neither propagated to nor updated with).  Padding slots carry
+ *   mask 0 and are copied through unchanged.
+ *
+ * Threading: a p2z_context belongs to one host thread at a time.  Device-side
+ * work is ordered on the stream passed in (or the context's own stream).
+ */
+#ifndef P2Z_H
+#define P2Z_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P2Z_ABI_VERSION 1
+
+/* Field constant of the reference's OMP/TBB/CUDA_v4 family:
+ * kfact = 100/(-0.299792458*3.8112) (src/propagate-toz-test_OMP.cpp:622),
+ * the 3.8 T solenoid.  p2z_config.kfact = 0 selects it. */
+#define P2Z_KFACT_DEFAULT (-87.5220642f)
+
+typedef enum p2z_status {
+  P2Z_OK = 0,
+  P2Z_BAD_ARG = 1,           /* invalid size, pointer or enum value */
+  P2Z_OOM = 2,               /* device or pinned-host allocation failed / budget exceeded */
+  P2Z_NONFINITE_INPUT = 3,   /* P2Z_FLAG_CHECK_INPUTS found a NaN/Inf in the inputs */
+  P2Z_SINGULAR = 4,          /* P2Z_FLAG_STRICT: a residual covariance had det <= 0 */
+  P2Z_TIMEOUT = 5,           /* a bounded wait ran out */
+  P2Z_CUDA_ERROR = 6,        /* a CUDA runtime call failed; see p2z_last_error() */
+  P2Z_NO_DEVICE = 7,         /* no usable CUDA device */
+  P2Z_UNSUPPORTED = 8,       /* valid but not built (e.g. an unsupported bsize) */
+  P2Z_NOT_READY = 9          /* serving: the request has not completed yet */
+} p2z_status;
+
+/* Measurement-update flavours.
+ *  V2            the reference's KalmanUpdate_v2 (src/propagate-toz-test_OMP.cpp:503-620):
+ *                2-D (x,y) update, FP32 with the 2x2 determinant and its reciprocal in FP64.
+ *  V2_COMP       the same estimator with no FP64: compensated (FMA error-free) FP32 determinant.
+ *  3X3_F64       3-D (x,y,z) update; the 3x3 residual covariance H C H^T + V is inverted and the
+ *                covariance is updated in the Joseph form (I-KH)C(I-KH)^T + KVK^T, both in FP64.
+ *                Basis: the reference's 3x3 KalmanUpdate (v1, :375-501), off its active path.
+ *  3X3_COMP      the 3-D Joseph update in FP32 only, with compensated cofactors/determinant.
+ *  F64           everything (propagation and V2 update) in FP64 on the GPU, for precision studies. */
+typedef enum p2z_update_kind {
+  P2Z_UPDATE_V2 = 0,
+  P2Z_UPDATE_V2_COMP = 1,
+  P2Z_UPDATE_3X3_F64 = 2,
+  P2Z_UPDATE_3X3_COMP = 3,
+  P2Z_UPDATE_F64 = 4
+} p2z_update_kind;
+
+/* How the work is laid onto the GPU.
+ *  AUTO        FLAT for uniform events, PERSISTENT when event_ntrks or a hit mask is given.
+ *  FLAT        one launch over every track slot of every event.
+ *  PER_EVENT   one launch per event (the reference's launch-per-chunk form,
+ *              src/propagate-toz-test_CUDA_v4.cu:970-986, taken down to one event per launch).
+ *  PERSISTENT  one persistent launch (grid = resident CTAs) whose warps take
+ *              32-slot work items from a device queue; replayed as a CUDA graph. */
+typedef enum p2z_schedule {
+  P2Z_SCHED_AUTO = 0,
+  P2Z_SCHED_FLAT = 1,
+  P2Z_SCHED_PER_EVENT = 2,
+  P2Z_SCHED_PERSISTENT = 3
+} p2z_schedule;
+
+/* Flags */
+#define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan inputs for NaN/Inf first -> P2Z_NONFINITE_INPUT */
+#define P2Z_FLAG_STRICT       0x2u  /* return P2Z_SINGULAR if any det <= 0 was met */
+#define P2Z_FLAG_NO_GRAPH     0x4u  /* PERSISTENT: launch directly instead of replaying a graph */
+#define P2Z_FLAG_ACCURATE_TRIG 0x8u /* sincosf for every angle (default: MUFU sin/cos for phi and
+                                       theta, a Taylor polynomial for the small angles alpha and
+                                       cosP*sina) */
+#define P2Z_FLAG_FULL_HITS    0x10u /* p2z_run: copy all 9 hit words per track even for the 2-D
+                                       updates (default: only the 6 words they read) */
+#define P2Z_FLAG_REFERENCE_ROUNDING 0x20u /* P2Z_UPDATE_V2 only: evaluate the reference's own FP32
+                                       expressions, type promotions and operation order, every
+                                       operation separately rounded, with correctly rounded
+                                       sin/cos -- the reference's results bit for bit where its
+                                       C library's sinf/cosf are correctly rounded.  Default: the
+                                       precise evaluation (versine form, wide x/y/phi
+                                       accumulators), within ~1e-6 of an FP64 evaluation. */
+
+typedef struct p2z_config {
+  int32_t abi_version;   /* must be P2Z_ABI_VERSION */
+  int32_t bsize;         /* AOSOA batch width B: 8, 16, 32 or 64 (reference macro bsize, :22-24) */
+  int64_t nevts;         /* number of events (reference macro nevts, :18-20) */
+  int64_t ntrks;         /* tracks per event, uniform form: a multiple of bsize
+                            (reference macro ntrks, nb = ntrks/bsize, :25-29); ignored
+                            when event_ntrks is given */
+  int32_t nlayer;        /* layers, 1..32 (reference macro nlayer, :35-37) */
+  int32_t niter;         /* passes over the whole input (reference NITER, :31-33); each pass
+                            recomputes the outputs from the inputs; 0 is treated as 1 */
+  float kfact;           /* 0 -> P2Z_KFACT_DEFAULT */
+  int32_t update;        /* p2z_update_kind */
+  int32_t schedule;      /* p2z_schedule */
+  int32_t block_threads; /* threads per CTA; 0 -> tuned default */
+  uint32_t flags;        /* P2Z_FLAG_* */
+  int32_t reserved0;
+  /* Uneven form (optional, host memory): nevts track counts.  NULL -> uniform. */
+  const int64_t *event_ntrks;
+} p2z_config;
+
+/* Filled by the run entry points (optional out-parameter). */
+typedef struct p2z_stats {
+  double kernel_ms;        /* device time of the hot-path launches (CUDA events), all iterations */
+  double h2d_ms;           /* host->device copy time (p2z_run only) */
+  double d2h_ms;           /* device->host copy time (p2z_run only) */
+  double total_ms;         /* device time from first copy to last copy */
+  int64_t track_slots;     /* slots processed per iteration (batches * bsize) */
+  int64_t updates;         /* track-layer updates performed per iteration (present hits) */
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+  int32_t launches;        /* hot-path kernel launches, all iterations */
+  int32_t singular;        /* 1 if a residual covariance with det <= 0 was met */
+} p2z_stats;
+
+typedef struct p2z_context p2z_context;
+
+/* ---- context -------------------------------------------------------------- */
+
+/* Create a context on CUDA device `device` (the current device when < 0).
+ * No counterpart in the reference (its main owns its device buffers directly,
+ * src/propagate-toz-test_CUDA_v4.cu:921-947). */
+p2z_status p2z_create(int device, p2z_context **out);
+p2z_status p2z_destroy(p2z_context *ctx);
+const char *p2z_status_string(p2z_status s);
+/* Last detailed error message of this context ("" if none); ctx may be NULL for
+ * the most recent context-free failure. */
+const char *p2z_last_error(const p2z_context *ctx);
+/* Library/ABI identification: returns P2Z_ABI_VERSION, fills a build string. */
+int p2z_version(char *buf, size_t buflen);
+
+/* ---- sizes ---------------------------------------------------------------- */
+
+/* Number of track batches described by cfg (uniform: nevts*ntrks/bsize; uneven:
+ * sum over events of ceil(n_e/bsize)); -1 on a bad config. */
+int64_t p2z_num_batches(const p2z_config *cfg);
+size_t p2z_sizeof_mptrk(int bsize);   /* 28*bsize*4 */
+size_t p2z_sizeof_mphit(int bsize);   /* 9*bsize*4 */
+
+/* ---- the hot path --------------------------------------------------------- */
+
+/* Full pass from HOST memory: copies tracks and hits to the device, runs
+ * propagateToZ + KalmanUpdate for every present layer of every track, copies
+ * the updated tracks back.  Replaces the reference's timed region in its
+ * include_data mode (src/propagate-toz-test_CUDA_v4.cu:966-990) and the CPU
+ * hot loop (src/propagate-toz-test_OMP.cpp:731-748).
+ *   trk_in   MPTRK[nbatches]            (host)
+ *   hits     MPHIT[nlayer*nbatches]     (host)
+ *   hit_mask uint32[nbatches*bsize]     (host, optional, see above)
+ *   trk_out  MPTRK[nbatches]            (host; may equal trk_in)
+ * Host buffers that are page-locked (cudaHostAlloc / p2z_host_alloc) are
+ * copied asynchronously; pageable ones go through a staging path. */
+p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, const void *hits,
+                   const uint32_t *hit_mask, void *trk_out, p2z_stats *stats);
+
+/* Same pass on DEVICE-resident buffers, enqueued on `stream` (a cudaStream_t;
+ * NULL = the context's stream).  Returns after enqueueing (asynchronous) unless
+ * stats != NULL, in which case it synchronises to fill the timings.
+ * d_trk_out must not alias d_trk_in.  Replaces GPUsequence/GPUsequenceR
+ * (src/propagate-toz-test_CUDA_v4.cu:746-828). */
+p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
+                          const uint32_t *d_hit_mask, void *d_trk_out, void *stream, p2z_stats *stats);
+
+/* One layer step on device buffers, in place on d_trk (nbatches MPTRK of width
+ * bsize): what = 1 propagateToZ (src/propagate-toz-test_OMP.cpp:623-682),
+ * 2 the measurement update selected by `update` (KalmanUpdate_v2, :503-620, for
+ * P2Z_UPDATE_V2), 3 both.  The hits used are those of `layer` in the standard
+ * hit array of nlayer layers.  Synchronous. */
+p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *d_trk, const void *d_hits,
+                           int nlayer, int layer, int what, int update, float kfact);
+
+/* ---- inputs (prepareTracks / prepareHits) ----------------------------------- */
+
+/* Seed structs, layout-identical to the reference's ATRK and AHIT
+ * (src/propagate-toz-test_OMP.cpp:57-67). */
+typedef struct p2z_atrk { float par[6]; float cov[21]; int32_t q; } p2z_atrk;
+typedef struct p2z_ahit { float pos[3]; float cov[6]; } p2z_ahit;
+
+/* The reference's input preparation: srand(1) (:715-718), then prepareTracks
+ * (:243-263) and prepareHits (:265-293), consuming the C library's rand()
+ * stream in the same order through the same polar-method randn (:127-145).
+ * Every element is multiplied by (1 + smear*N(0,1)); covariance elements are
+ * further multiplied by cov_scale (the reference uses 100); charge is copied.
+ * Layer l uses hit seed l; nseeds < nlayer is P2Z_BAD_ARG (the reference exits).
+ * With smear = 1e-7 and cov_scale = 100 the output is bit-identical to the
+ * reference's.  Host memory; trk_out holds nevts*ntrks/bsize MPTRK, hits_out
+ * nlayer*nevts*ntrks/bsize MPHIT.  Uses a private generator state (the global
+ * rand() state is not touched) so concurrent calls are safe. */
+p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
+                       int64_t ntrks, int nlayer, double smear, double cov_scale, void *trk_out, void *hits_out);
+
+/* Physics workload generator (no counterpart in the reference): tracks of
+ * charge +-1, pT log-uniform in [pt_min, pt_max] GeV, phi ~ U(-pi, pi),
+ * eta ~ U(eta_min, eta_max), vertex z ~ N(0, sigma_vz); covariance
+ * diag(sigma) * random correlation (|rho| <= rho_max, positive definite) * diag(sigma)
+ * with sigma = (sig_xy, sig_xy, sig_z, rel_sig_ipt*ipt, sig_phi, sig_theta); the
+ * initial parameters are the truth smeared with that covariance.  Hits on nlayer
+ * planes z_first..z_last at the true helix point (the propagateToZ helix with
+ * the same kfact, evaluated in FP64) plus Gaussian noise (hit_sig_xy, hit_sig_z)
+ * with a diagonal 3x3 covariance.  Counter-based RNG: output depends only on
+ * (seed, track index), independent of threading.  Uniform or uneven events
+ * (event_ntrks != NULL); hit_mask (optional) receives all-present masks for
+ * real tracks and 0 for padding slots. */
+typedef struct p2z_physics_params {
+  uint64_t seed;
+  double pt_min, pt_max, eta_min, eta_max, sigma_vz;
+  double sig_xy, sig_z, rel_sig_ipt, sig_phi, sig_theta, rho_max;
+  double z_first, z_last;
+  double hit_sig_xy, hit_sig_z;
+  float kfact;  /* 0 -> default */
+  int32_t nthreads; /* host threads; 0 -> all */
+} p2z_physics_params;
+void p2z_physics_defaults(p2z_physics_params *p);
+p2z_status p2z_generate_physics(const p2z_physics_params *p, const p2z_config *cfg, void *trk_out, void *hits_out,
+                                uint32_t *hit_mask);
+
+/* Drop layers from a hit mask (no counterpart in the reference): each real
+ * track (mask != 0) keeps a contiguous run of L layers starting at layer 0 with
+ * L uniform in [min_hits, max_hits], then loses each layer independently with
+ * probability drop_prob as long as at least min_hits remain.  Deterministic in
+ * (seed, slot). */
+p2z_status p2z_mask_layers(uint32_t *hit_mask, int64_t nslots, int nlayer, int min_hits, int max_hits,
+                           double drop_prob, uint64_t seed);
+
+/* ---- validation block ------------------------------------------------------- */
+
+/* Accumulators of the reference's printed validation block
+ * (src/propagate-toz-test_OMP.cpp:758-876). */
+typedef struct p2z_validation {
+  double avgx, avgy, avgz, avgdx, avgdy, avgdz, avgpt, avgphi, avgtheta;
+  double stdx, stdy, stdz, stddx, stddy, stddz;
+  int64_t nnans, nfail, ngood;
+} p2z_validation;
+
+/* Compute the block over nevts*ntrks output tracks against the last-layer
+ * seed hit (hx, hy, hz), with the reference's NaN test, its "fail" window
+ * (pt~12, phi~1.3, theta~2.8, :784-795) and its divisions by ngood. */
+p2z_status p2z_validate(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
+                        p2z_validation *v);
+/* Print it with the reference's exact format (:866-876) to stdout. */
+void p2z_print_validation(const p2z_validation *v);
+/* The machine-readable line of the reference (:756), parsed by its tools
+ * (tools/compare.py:12): "formatted NITER nevts ntrks bsize nb wall 0 setup nthreads". */
+void p2z_print_formatted(int niter, int64_t nevts, int64_t ntrks, int bsize, double wall_s, double setup_s,
+                         int nthreads);
+
+/* ---- host memory helpers ---------------------------------------------------- */
+
+/* Page-locked host allocation (cudaHostAlloc) for fast asynchronous copies. */
+p2z_status p2z_host_alloc(void **ptr, size_t bytes);
+p2z_status p2z_host_free(void *ptr);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* P2Z_H */

@@ -1,0 +1,371 @@
+"""Python binding of libp2z.so, the B200 propagate-to-z + Kalman-update library.
+
+The product is the shared library built from ``csrc/`` (sm_100a kernels and the
+``extern "C"`` boundary declared in ``include/p2z.h``).  This module only binds
+that C ABI with ctypes for tests, benchmarks and Python callers; it has no
+compute path of its own.  Importing it fails loudly when the library has not
+been built -- there is no fallback.
+
+Layout helpers use numpy views of the reference's AOSOA structs
+(src/propagate-toz-test_OMP.cpp:57-125): a track batch of width B is
+``par[6*B] cov[21*B] q[B]`` (28*B 32-bit words), a hit batch ``pos[3*B] cov[6*B]``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libp2z.so"
+INCLUDE_H = PKG_DIR.parent / "include" / "p2z.h"
+
+ABI_VERSION = 1
+KFACT_DEFAULT = np.float32(100.0 / (-0.299792458 * 3.8112))
+TRK_WORDS = 28
+HIT_WORDS = 9
+
+# status codes
+OK, BAD_ARG, OOM, NONFINITE_INPUT, SINGULAR, TIMEOUT, CUDA_ERROR, NO_DEVICE, UNSUPPORTED, NOT_READY = range(10)
+STATUS_NAMES = ["OK", "BAD_ARG", "OOM", "NONFINITE_INPUT", "SINGULAR", "TIMEOUT", "CUDA_ERROR", "NO_DEVICE",
+                "UNSUPPORTED", "NOT_READY"]
+# update kinds
+UPDATE_V2, UPDATE_V2_COMP, UPDATE_3X3_F64, UPDATE_3X3_COMP, UPDATE_F64 = range(5)
+UPDATE_NAMES = {"v2": UPDATE_V2, "v2_comp": UPDATE_V2_COMP, "3x3_f64": UPDATE_3X3_F64,
+                "3x3_comp": UPDATE_3X3_COMP, "f64": UPDATE_F64}
+# schedules
+SCHED_AUTO, SCHED_FLAT, SCHED_PER_EVENT, SCHED_PERSISTENT = range(4)
+SCHED_NAMES = {"auto": SCHED_AUTO, "flat": SCHED_FLAT, "per_event": SCHED_PER_EVENT,
+               "persistent": SCHED_PERSISTENT}
+# flags
+FLAG_CHECK_INPUTS = 0x1
+FLAG_STRICT = 0x2
+FLAG_NO_GRAPH = 0x4
+FLAG_ACCURATE_TRIG = 0x8
+FLAG_FULL_HITS = 0x10
+
+
+class P2zError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"p2z {name}: {msg}")
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("bsize", C.c_int32), ("nevts", C.c_int64), ("ntrks", C.c_int64),
+                ("nlayer", C.c_int32), ("niter", C.c_int32), ("kfact", C.c_float), ("update", C.c_int32),
+                ("schedule", C.c_int32), ("block_threads", C.c_int32), ("flags", C.c_uint32),
+                ("reserved0", C.c_int32), ("event_ntrks", C.POINTER(C.c_int64))]
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_double), ("h2d_ms", C.c_double), ("d2h_ms", C.c_double),
+                ("total_ms", C.c_double), ("track_slots", C.c_int64), ("updates", C.c_int64),
+                ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("launches", C.c_int32),
+                ("singular", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Atrk(C.Structure):
+    _fields_ = [("par", C.c_float * 6), ("cov", C.c_float * 21), ("q", C.c_int32)]
+
+
+class Ahit(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("cov", C.c_float * 6)]
+
+
+class PhysicsParams(C.Structure):
+    _fields_ = [("seed", C.c_uint64)] + [(n, C.c_double) for n in (
+        "pt_min", "pt_max", "eta_min", "eta_max", "sigma_vz", "sig_xy", "sig_z", "rel_sig_ipt", "sig_phi",
+        "sig_theta", "rho_max", "z_first", "z_last", "hit_sig_xy", "hit_sig_z")] + [
+        ("kfact", C.c_float), ("nthreads", C.c_int32)]
+
+
+class Validation(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("avgx", "avgy", "avgz", "avgdx", "avgdy", "avgdz", "avgpt", "avgphi",
+                                          "avgtheta", "stdx", "stdy", "stdz", "stddx", "stddy", "stddz")] + [
+        ("nnans", C.c_int64), ("nfail", C.c_int64), ("ngood", C.c_int64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+# Every symbol include/p2z.h declares, with its ctypes signature.
+_VP, _CVP = C.c_void_p, C.c_void_p
+_SIGS = {
+    "p2z_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "p2z_destroy": (C.c_int, [_VP]),
+    "p2z_status_string": (C.c_char_p, [C.c_int]),
+    "p2z_last_error": (C.c_char_p, [_VP]),
+    "p2z_version": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "p2z_num_batches": (C.c_int64, [C.POINTER(Config)]),
+    "p2z_sizeof_mptrk": (C.c_size_t, [C.c_int]),
+    "p2z_sizeof_mphit": (C.c_size_t, [C.c_int]),
+    "p2z_run": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, _VP, C.POINTER(Stats)]),
+    "p2z_run_device": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP, C.POINTER(Stats)]),
+    "p2z_step_device": (C.c_int, [_VP, C.c_int, C.c_int64, _VP, _CVP, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_float]),
+    "p2z_prepare": (C.c_int, [C.POINTER(Atrk), C.POINTER(Ahit), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int,
+                              C.c_double, C.c_double, _VP, _VP]),
+    "p2z_physics_defaults": (None, [C.POINTER(PhysicsParams)]),
+    "p2z_generate_physics": (C.c_int, [C.POINTER(PhysicsParams), C.POINTER(Config), _VP, _VP, _VP]),
+    "p2z_mask_layers": (C.c_int, [_VP, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64]),
+    "p2z_validate": (C.c_int, [_CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float), C.POINTER(Validation)]),
+    "p2z_print_validation": (None, [C.POINTER(Validation)]),
+    "p2z_print_formatted": (None, [C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int]),
+    "p2z_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
+    "p2z_host_free": (C.c_int, [_VP]),
+}
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `make -C {PKG_DIR}` or __graft_entry__.build()")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/p2z.h (parsed from the header)."""
+    import re
+    text = INCLUDE_H.read_text()
+    return sorted(set(re.findall(r"\b(p2z_[a-z0-9_]+)\s*\(", text)))
+
+
+def _check(status: int, ctx=None):
+    if status != OK:
+        msg = lib.p2z_last_error(ctx)
+        raise P2zError(status, (msg or b"").decode())
+
+
+def version() -> str:
+    buf = C.create_string_buffer(256)
+    lib.p2z_version(buf, 256)
+    return buf.value.decode()
+
+
+# ---------------------------------------------------------------------------
+# AOSOA helpers
+# ---------------------------------------------------------------------------
+
+def trk_words(bsize: int) -> int:
+    return TRK_WORDS * bsize
+
+
+def hit_words(bsize: int) -> int:
+    return HIT_WORDS * bsize
+
+
+def empty_tracks(nbatches: int, bsize: int) -> np.ndarray:
+    """float32 array of nbatches MPTRK batches (charge words hold int32 bits)."""
+    return np.zeros((nbatches, TRK_WORDS, bsize), dtype=np.float32)
+
+
+def empty_hits(nbatches: int, nlayer: int, bsize: int) -> np.ndarray:
+    return np.zeros((nbatches, nlayer, HIT_WORDS, bsize), dtype=np.float32)
+
+
+def tracks_to_aos(trk: np.ndarray) -> dict:
+    """(nbatches, 28, B) AOSOA -> per-track arrays in slot order: par (n,6), cov (n,21), q (n,)."""
+    nb, w, B = trk.shape
+    assert w == TRK_WORDS
+    t = np.ascontiguousarray(trk.transpose(0, 2, 1)).reshape(nb * B, TRK_WORDS)
+    return {"par": t[:, :6].copy(), "cov": t[:, 6:27].copy(), "q": t[:, 27].copy().view(np.int32)}
+
+
+def hits_to_aos(hits: np.ndarray) -> dict:
+    """(nbatches, nlayer, 9, B) -> pos (nslots, nlayer, 3), cov (nslots, nlayer, 6)."""
+    nb, nl, w, B = hits.shape
+    h = np.ascontiguousarray(hits.transpose(0, 3, 1, 2)).reshape(nb * B, nl, HIT_WORDS)
+    return {"pos": h[:, :, :3].copy(), "cov": h[:, :, 3:].copy()}
+
+
+def make_config(bsize=32, nevts=1, ntrks=None, nlayer=20, niter=1, kfact=0.0, update=UPDATE_V2,
+                schedule=SCHED_AUTO, block_threads=0, flags=0, event_ntrks=None):
+    cfg = Config()
+    cfg.abi_version = ABI_VERSION
+    cfg.bsize = bsize
+    cfg.nevts = nevts
+    cfg.ntrks = ntrks if ntrks is not None else bsize
+    cfg.nlayer = nlayer
+    cfg.niter = niter
+    cfg.kfact = kfact
+    cfg.update = UPDATE_NAMES.get(update, update) if isinstance(update, str) else update
+    cfg.schedule = SCHED_NAMES.get(schedule, schedule) if isinstance(schedule, str) else schedule
+    cfg.block_threads = block_threads
+    cfg.flags = flags
+    if event_ntrks is not None:
+        arr = np.ascontiguousarray(event_ntrks, dtype=np.int64)
+        cfg._event_ntrks_keep = arr  # keep alive with the struct
+        cfg.event_ntrks = arr.ctypes.data_as(C.POINTER(C.c_int64))
+    return cfg
+
+
+def num_batches(cfg: Config) -> int:
+    n = lib.p2z_num_batches(C.byref(cfg))
+    if n < 0:
+        _check(BAD_ARG, None)
+    return n
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+# ---------------------------------------------------------------------------
+# Inputs and validation (host)
+# ---------------------------------------------------------------------------
+
+def make_atrk(par, cov, q) -> Atrk:
+    t = Atrk()
+    t.par[:] = [float(v) for v in par]
+    t.cov[:] = [float(v) for v in cov]
+    t.q = int(q)
+    return t
+
+
+def make_ahits(hits) -> C.Array:
+    arr = (Ahit * len(hits))()
+    for i, (pos, cov) in enumerate(hits):
+        arr[i].pos[:] = [float(v) for v in pos]
+        arr[i].cov[:] = [float(v) for v in cov]
+    return arr
+
+
+def prepare(seed: Atrk, hit_seeds, bsize, nevts, ntrks, nlayer, smear=1e-7, cov_scale=100.0):
+    """The reference's srand(1) + prepareTracks + prepareHits (AOSOA numpy arrays)."""
+    nb = nevts * (ntrks // bsize)
+    trk = empty_tracks(nb, bsize)
+    hit = empty_hits(nb, nlayer, bsize)
+    _check(lib.p2z_prepare(C.byref(seed), hit_seeds, len(hit_seeds), bsize, nevts, ntrks, nlayer, smear, cov_scale,
+                           _ptr(trk), _ptr(hit)))
+    return trk, hit
+
+
+def physics_params(**kw) -> PhysicsParams:
+    p = PhysicsParams()
+    lib.p2z_physics_defaults(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def generate_physics(cfg: Config, params: PhysicsParams | None = None, with_mask=False, out=None):
+    """Physics workload into (trk, hits[, mask]) numpy arrays (or into `out`)."""
+    params = params or physics_params()
+    nb = num_batches(cfg)
+    if out is None:
+        trk = empty_tracks(nb, cfg.bsize)
+        hit = empty_hits(nb, cfg.nlayer, cfg.bsize)
+        mask = np.zeros(nb * cfg.bsize, dtype=np.uint32) if with_mask else None
+    else:
+        trk, hit, mask = out
+    _check(lib.p2z_generate_physics(C.byref(params), C.byref(cfg), _ptr(trk), _ptr(hit), _ptr(mask)))
+    return (trk, hit, mask) if with_mask else (trk, hit)
+
+
+def mask_layers(mask: np.ndarray, nlayer, min_hits=5, max_hits=20, drop_prob=0.1, seed=7):
+    _check(lib.p2z_mask_layers(_ptr(mask), mask.size, nlayer, min_hits, max_hits, drop_prob, seed))
+    return mask
+
+
+def validate(trk_out: np.ndarray, bsize, nevts, ntrks, hit_last) -> dict:
+    v = Validation()
+    hl = (C.c_float * 3)(*[float(x) for x in hit_last])
+    _check(lib.p2z_validate(_ptr(trk_out), bsize, nevts, ntrks, hl, C.byref(v)))
+    return v
+
+
+def print_validation(v: Validation):
+    lib.p2z_print_validation(C.byref(v))
+
+
+# ---------------------------------------------------------------------------
+# Context
+# ---------------------------------------------------------------------------
+
+class Context:
+    """Owns a p2z_context (device buffers, streams, graph cache) on one GPU."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib.p2z_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.p2z_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, cfg: Config, trk_in, hits, trk_out, hit_mask=None) -> Stats:
+        """Host-memory pass (copies in, kernels, copies out)."""
+        st = Stats()
+        _check(lib.p2z_run(self.h, C.byref(cfg), _ptr(trk_in), _ptr(hits), _ptr(hit_mask), _ptr(trk_out),
+                           C.byref(st)), self.h)
+        return st
+
+    def run_device(self, cfg: Config, d_trk_in, d_hits, d_trk_out, d_mask=None, stream=None, stats=True):
+        """Device-memory pass; pointers are ints or objects with data_ptr()."""
+        st = Stats() if stats else None
+        _check(lib.p2z_run_device(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits), _ptr(d_mask),
+                                  _ptr(d_trk_out), stream, C.byref(st) if st is not None else None), self.h)
+        return st
+
+    def step_device(self, bsize, nbatches, d_trk, d_hits, nlayer, layer, what=3, update=UPDATE_V2, kfact=0.0):
+        _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
+                                   kfact), self.h)
+
+
+class PinnedArray:
+    """numpy view of page-locked host memory from p2z_host_alloc."""
+
+    def __init__(self, shape, dtype=np.float32):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = C.c_void_p()
+        _check(lib.p2z_host_alloc(C.byref(p), n))
+        self._p = p
+        buf = (C.c_char * n).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self._p:
+            self.array = None
+            lib.p2z_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -1,0 +1,657 @@
+// p2z_api.cu -- the extern "C" boundary (include/p2z.h): contexts, the hot-path
+// run entry points, launch scheduling (flat / per-event / persistent replayed
+// as a CUDA graph) and host<->device copy pipelining.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "p2z.h"
+#include "p2z_kernels.cuh"
+
+namespace p2z {
+cudaError_t launch_step(int bsize, float *trk, const float *hits, int64_t nslots, int nlayer, int layer, int what,
+                        float kfact, cudaStream_t st);
+}
+
+using namespace p2z;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_last_error;  // failures with no context
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct GraphKey {
+  RunArgs args;
+  int bsize, upd, sc, block, grid;
+  bool masked;
+  bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+};
+
+}  // namespace
+
+struct p2z_context {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t copy[2] = {nullptr, nullptr};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  cudaEvent_t join[2] = {nullptr, nullptr};
+  unsigned int *d_status = nullptr;         // device status word
+  unsigned long long *d_queue = nullptr;    // 2 persistent work counters (one per copy stream)
+  DevBuf trk, hits, out, mask, valid;       // p2z_run buffers / internal masks
+  bool has_graph = false;
+  GraphKey gkey;
+  cudaGraphExec_t gexec = nullptr;
+  std::string last_error;
+};
+
+namespace {
+
+p2z_status fail(p2z_context *ctx, p2z_status st, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) {
+    ctx->last_error = buf;
+  } else {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_last_error = buf;
+  }
+  return st;
+}
+
+#define P2Z_CUDA(ctx, call)                                                                          \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return fail((ctx), e_ == cudaErrorMemoryAllocation ? P2Z_OOM : P2Z_CUDA_ERROR, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                \
+  } while (0)
+
+p2z_status ensure(p2z_context *ctx, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes) return P2Z_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  if (bytes == 0) return P2Z_OK;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, P2Z_OOM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  b.bytes = bytes;
+  return P2Z_OK;
+}
+
+bool valid_bsize(int b) { return b == 8 || b == 16 || b == 32 || b == 64; }
+
+// Validated view of a config.
+struct Plan {
+  int B = 0;
+  int nlayer = 0;
+  int niter = 1;
+  float kfact = 0.f;
+  int upd = 0;
+  int sc = SC_FAST;
+  int schedule = P2Z_SCHED_FLAT;
+  int block = 0;
+  uint32_t flags = 0;
+  int64_t nbatches = 0;
+  int64_t nslots = 0;
+  bool uneven = false;
+  std::vector<int64_t> ev_slot_begin;  // nevts + 1 entries
+  std::vector<uint8_t> batch_valid;    // uneven: real lanes per batch
+};
+
+p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
+  if (!cfg) return fail(ctx, P2Z_BAD_ARG, "config is NULL");
+  if (cfg->abi_version != P2Z_ABI_VERSION)
+    return fail(ctx, P2Z_BAD_ARG, "abi_version %d != %d", cfg->abi_version, P2Z_ABI_VERSION);
+  if (!valid_bsize(cfg->bsize)) return fail(ctx, P2Z_UNSUPPORTED, "bsize %d not in {8,16,32,64}", cfg->bsize);
+  if (cfg->nlayer < 1 || cfg->nlayer > 32) return fail(ctx, P2Z_BAD_ARG, "nlayer %d not in 1..32", cfg->nlayer);
+  if (cfg->nevts < 0) return fail(ctx, P2Z_BAD_ARG, "nevts %lld < 0", (long long)cfg->nevts);
+  if (cfg->update < P2Z_UPDATE_V2 || cfg->update > P2Z_UPDATE_F64)
+    return fail(ctx, P2Z_BAD_ARG, "update kind %d unknown", cfg->update);
+  if (cfg->schedule < P2Z_SCHED_AUTO || cfg->schedule > P2Z_SCHED_PERSISTENT)
+    return fail(ctx, P2Z_BAD_ARG, "schedule %d unknown", cfg->schedule);
+  if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
+    return fail(ctx, P2Z_BAD_ARG, "block_threads %d not a multiple of 32 in 32..256", cfg->block_threads);
+  pl.B = cfg->bsize;
+  pl.nlayer = cfg->nlayer;
+  pl.niter = cfg->niter > 0 ? cfg->niter : 1;
+  pl.kfact = cfg->kfact != 0.f ? cfg->kfact : (float)(100. / (-0.299792458 * 3.8112));
+  pl.upd = cfg->update;
+  pl.flags = cfg->flags;
+  if (cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING) {
+    if (cfg->update != P2Z_UPDATE_V2)
+      return fail(ctx, P2Z_UNSUPPORTED, "P2Z_FLAG_REFERENCE_ROUNDING applies to P2Z_UPDATE_V2 only");
+    pl.upd = UPDK_V2_REF;
+  }
+  pl.sc = (cfg->flags & P2Z_FLAG_ACCURATE_TRIG) ? SC_ACCURATE : SC_FAST;
+  pl.block = cfg->block_threads ? cfg->block_threads : 128;
+  pl.ev_slot_begin.assign((size_t)cfg->nevts + 1, 0);
+  if (cfg->event_ntrks) {
+    pl.uneven = true;
+    int64_t nb = 0;
+    for (int64_t e = 0; e < cfg->nevts; ++e) {
+      const int64_t n = cfg->event_ntrks[e];
+      if (n < 0) return fail(ctx, P2Z_BAD_ARG, "event_ntrks[%lld] = %lld < 0", (long long)e, (long long)n);
+      pl.ev_slot_begin[e] = nb * pl.B;
+      const int64_t nbe = (n + pl.B - 1) / pl.B;
+      for (int64_t i = 0; i < nbe; ++i) {
+        const int64_t left = n - i * pl.B;
+        pl.batch_valid.push_back((uint8_t)(left >= pl.B ? pl.B : left));
+      }
+      nb += nbe;
+    }
+    pl.nbatches = nb;
+    pl.ev_slot_begin[cfg->nevts] = nb * pl.B;
+  } else {
+    if (cfg->ntrks < 0 || cfg->ntrks % cfg->bsize)
+      return fail(ctx, P2Z_BAD_ARG, "ntrks %lld is not a non-negative multiple of bsize %d", (long long)cfg->ntrks,
+                  cfg->bsize);
+    pl.nbatches = cfg->nevts * (cfg->ntrks / cfg->bsize);
+    for (int64_t e = 0; e <= cfg->nevts; ++e) pl.ev_slot_begin[e] = e * cfg->ntrks;
+  }
+  pl.nslots = pl.nbatches * pl.B;
+  pl.schedule = cfg->schedule;
+  return P2Z_OK;
+}
+
+cudaError_t dispatch(const LaunchSpec &s, cudaStream_t st) {
+  switch (s.upd) {
+    case UPDK_V2: return launch_v2(s, st);
+    case UPDK_V2_COMP: return launch_v2_comp(s, st);
+    case UPDK_3X3_F64: return launch_3x3_f64(s, st);
+    case UPDK_3X3_COMP: return launch_3x3_comp(s, st);
+    case UPDK_F64: return launch_f64(s, st);
+    case UPDK_V2_REF: return launch_v2_ref(s, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int occupancy(const LaunchSpec &s) {
+  switch (s.upd) {
+    case UPDK_V2: return occupancy_v2(s);
+    case UPDK_V2_COMP: return occupancy_v2_comp(s);
+    case UPDK_3X3_F64: return occupancy_3x3_f64(s);
+    case UPDK_3X3_COMP: return occupancy_3x3_comp(s);
+    case UPDK_F64: return occupancy_f64(s);
+    case UPDK_V2_REF: return occupancy_v2_ref(s);
+  }
+  return 0;
+}
+
+// Writes masks for uneven events: all layers for real lanes, 0 for padding.
+__global__ void k_fill_mask(uint32_t *mask, const uint8_t *valid, int64_t nslots, int B, uint32_t all) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  mask[s] = ((int)(s % B) < (int)valid[s / B]) ? all : 0u;
+}
+
+// Sum of popcounts of the masks (track-layer updates requested).
+__global__ void k_count_updates(const uint32_t *mask, int64_t nslots, uint32_t all, unsigned long long *out) {
+  unsigned long long acc = 0;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += (int64_t)gridDim.x * blockDim.x)
+    acc += __popc(mask[s] & all);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
+uint32_t all_layers(int nlayer) { return nlayer >= 32 ? 0xffffffffu : ((1u << nlayer) - 1u); }
+
+// Enqueue the hot-path launches of one pass over slots [s0, s1) on st.
+// queue: the persistent work counter to use.
+p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, int64_t s0, int64_t s1,
+                        int schedule, cudaStream_t st, unsigned long long *queue, int *launches) {
+  LaunchSpec spec;
+  spec.args = base;
+  spec.args.queue = queue;
+  spec.bsize = pl.B;
+  spec.upd = pl.upd;
+  spec.sc = pl.sc;
+  spec.masked = base.mask != nullptr;
+  spec.block = pl.block;
+  spec.grid = 0;
+  if (schedule == P2Z_SCHED_PER_EVENT) {
+    spec.kind = KIND_FLAT;
+    const int64_t nev = (int64_t)pl.ev_slot_begin.size() - 1;
+    for (int64_t e = 0; e < nev; ++e) {
+      const int64_t a = std::max(s0, pl.ev_slot_begin[e]), b = std::min(s1, pl.ev_slot_begin[e + 1]);
+      if (b <= a) continue;
+      spec.args.slot_begin = a;
+      spec.args.slot_end = b;
+      P2Z_CUDA(ctx, dispatch(spec, st));
+      ++*launches;
+    }
+    return P2Z_OK;
+  }
+  spec.args.slot_begin = s0;
+  spec.args.slot_end = s1;
+  if (s1 <= s0) return P2Z_OK;
+  if (schedule == P2Z_SCHED_FLAT) {
+    spec.kind = KIND_FLAT;
+    P2Z_CUDA(ctx, dispatch(spec, st));
+    ++*launches;
+    return P2Z_OK;
+  }
+  // persistent
+  spec.kind = KIND_PERSISTENT;
+  const int occ = occupancy(spec);
+  if (occ <= 0) return fail(ctx, P2Z_CUDA_ERROR, "occupancy query failed for the persistent kernel");
+  const int64_t items = (s1 - s0 + 31) / 32;
+  const int64_t warps_per_cta = spec.block / 32;
+  spec.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * ctx->num_sms, (items + warps_per_cta - 1) / warps_per_cta));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  P2Z_CUDA(ctx, cudaStreamIsCapturing(st, &cap));
+  const bool use_graph = !(pl.flags & P2Z_FLAG_NO_GRAPH) && cap == cudaStreamCaptureStatusNone;
+  if (!use_graph) {
+    P2Z_CUDA(ctx, cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
+    P2Z_CUDA(ctx, dispatch(spec, st));
+    ++*launches;
+    return P2Z_OK;
+  }
+  GraphKey key;
+  std::memset(&key, 0, sizeof key);
+  key.args = spec.args;
+  key.bsize = spec.bsize;
+  key.upd = spec.upd;
+  key.sc = spec.sc;
+  key.block = spec.block;
+  key.grid = spec.grid;
+  key.masked = spec.masked;
+  if (!(ctx->has_graph && ctx->gkey == key)) {
+    if (ctx->gexec) {
+      cudaGraphExecDestroy(ctx->gexec);
+      ctx->gexec = nullptr;
+    }
+    ctx->has_graph = false;
+    cudaGraph_t g = nullptr;
+    P2Z_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
+    cudaError_t e2 = dispatch(spec, st);
+    cudaError_t e3 = cudaStreamEndCapture(st, &g);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return fail(ctx, P2Z_CUDA_ERROR, "graph capture of the persistent launch failed: %s / %s / %s",
+                  cudaGetErrorString(e1), cudaGetErrorString(e2), cudaGetErrorString(e3));
+    }
+    cudaError_t e4 = cudaGraphInstantiate(&ctx->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e4 != cudaSuccess) return fail(ctx, P2Z_CUDA_ERROR, "cudaGraphInstantiate: %s", cudaGetErrorString(e4));
+    ctx->gkey = key;
+    ctx->has_graph = true;
+  }
+  P2Z_CUDA(ctx, cudaGraphLaunch(ctx->gexec, st));
+  ++*launches;
+  return P2Z_OK;
+}
+
+int resolve_schedule(const Plan &pl, bool masked) {
+  if (pl.schedule != P2Z_SCHED_AUTO) return pl.schedule;
+  return (pl.uneven || masked) ? P2Z_SCHED_PERSISTENT : P2Z_SCHED_FLAT;
+}
+
+// Builds the padding mask of uneven events into ctx->valid / ctx->mask.
+p2z_status internal_mask(p2z_context *ctx, const Plan &pl, cudaStream_t st, const uint32_t **out) {
+  p2z_status r = ensure(ctx, ctx->valid, pl.batch_valid.size());
+  if (r != P2Z_OK) return r;
+  r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots);
+  if (r != P2Z_OK) return r;
+  if (pl.nslots == 0) {
+    *out = (const uint32_t *)ctx->mask.p;
+    return P2Z_OK;
+  }
+  P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->valid.p, pl.batch_valid.data(), pl.batch_valid.size(), cudaMemcpyHostToDevice, st));
+  k_fill_mask<<<(unsigned)((pl.nslots + 255) / 256), 256, 0, st>>>((uint32_t *)ctx->mask.p, (const uint8_t *)ctx->valid.p,
+                                                                   pl.nslots, pl.B, all_layers(pl.nlayer));
+  P2Z_CUDA(ctx, cudaGetLastError());
+  *out = (const uint32_t *)ctx->mask.p;
+  return P2Z_OK;
+}
+
+p2z_status count_updates(p2z_context *ctx, const Plan &pl, const uint32_t *d_mask, cudaStream_t st, int64_t *out) {
+  if (!d_mask) {
+    *out = pl.nslots * pl.nlayer;
+    return P2Z_OK;
+  }
+  if (pl.nslots == 0) {
+    *out = 0;
+    return P2Z_OK;
+  }
+  unsigned long long *d = ctx->d_queue + 2;  // scratch word
+  P2Z_CUDA(ctx, cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
+  k_count_updates<<<ctx->num_sms * 4, 256, 0, st>>>(d_mask, pl.nslots, all_layers(pl.nlayer), d);
+  P2Z_CUDA(ctx, cudaGetLastError());
+  unsigned long long h = 0;
+  P2Z_CUDA(ctx, cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, st));
+  P2Z_CUDA(ctx, cudaStreamSynchronize(st));
+  *out = (int64_t)h;
+  return P2Z_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *p2z_status_string(p2z_status s) {
+  switch (s) {
+    case P2Z_OK: return "ok";
+    case P2Z_BAD_ARG: return "bad argument";
+    case P2Z_OOM: return "out of memory";
+    case P2Z_NONFINITE_INPUT: return "non-finite input";
+    case P2Z_SINGULAR: return "singular residual covariance";
+    case P2Z_TIMEOUT: return "timeout";
+    case P2Z_CUDA_ERROR: return "CUDA error";
+    case P2Z_NO_DEVICE: return "no CUDA device";
+    case P2Z_UNSUPPORTED: return "unsupported";
+    case P2Z_NOT_READY: return "not ready";
+  }
+  return "unknown status";
+}
+
+const char *p2z_last_error(const p2z_context *ctx) {
+  if (ctx) return ctx->last_error.c_str();
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return g_last_error.c_str();
+}
+
+int p2z_version(char *buf, size_t buflen) {
+  if (buf && buflen) {
+    std::snprintf(buf, buflen, "libp2z abi %d, sm_100a, built %s %s, CUDA %d", P2Z_ABI_VERSION, __DATE__, __TIME__,
+                  CUDART_VERSION);
+  }
+  return P2Z_ABI_VERSION;
+}
+
+size_t p2z_sizeof_mptrk(int bsize) { return valid_bsize(bsize) ? (size_t)TRK_WORDS * bsize * 4 : 0; }
+size_t p2z_sizeof_mphit(int bsize) { return valid_bsize(bsize) ? (size_t)HIT_WORDS * bsize * 4 : 0; }
+
+int64_t p2z_num_batches(const p2z_config *cfg) {
+  Plan pl;
+  if (make_plan(nullptr, cfg, pl) != P2Z_OK) return -1;
+  return pl.nbatches;
+}
+
+p2z_status p2z_create(int device, p2z_context **out) {
+  if (!out) return fail(nullptr, P2Z_BAD_ARG, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(nullptr, P2Z_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  if (device < 0) {
+    if (cudaGetDevice(&device) != cudaSuccess) return fail(nullptr, P2Z_NO_DEVICE, "cudaGetDevice failed");
+  }
+  if (device >= ndev) return fail(nullptr, P2Z_BAD_ARG, "device %d >= device count %d", device, ndev);
+  p2z_context *c = new p2z_context();
+  c->device = device;
+  auto bail = [&](const char *what, cudaError_t err) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(err);
+    p2z_destroy(c);
+    return fail(nullptr, err == cudaErrorMemoryAllocation ? P2Z_OOM : P2Z_CUDA_ERROR, "%s", msg.c_str());
+  };
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return bail("cudaSetDevice", e);
+  if ((e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+    return bail("cudaDeviceGetAttribute", e);
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail("stream", e);
+  for (int i = 0; i < 2; ++i) {
+    if ((e = cudaStreamCreateWithFlags(&c->copy[i], cudaStreamNonBlocking)) != cudaSuccess) return bail("stream", e);
+    if ((e = cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming)) != cudaSuccess) return bail("event", e);
+  }
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return bail("event", e);
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return bail("event", e);
+  if ((e = cudaEventCreate(&c->ev2)) != cudaSuccess) return bail("event", e);
+  if ((e = cudaEventCreate(&c->ev3)) != cudaSuccess) return bail("event", e);
+  if ((e = cudaMalloc(&c->d_status, sizeof(unsigned int))) != cudaSuccess) return bail("cudaMalloc status", e);
+  if ((e = cudaMalloc(&c->d_queue, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail("cudaMalloc queue", e);
+  if ((e = cudaMemset(c->d_status, 0, sizeof(unsigned int))) != cudaSuccess) return bail("cudaMemset", e);
+  *out = c;
+  return P2Z_OK;
+}
+
+p2z_status p2z_destroy(p2z_context *c) {
+  if (!c) return P2Z_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < 2; ++i)
+    if (c->copy[i]) cudaStreamSynchronize(c->copy[i]);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  for (DevBuf *b : {&c->trk, &c->hits, &c->out, &c->mask, &c->valid})
+    if (b->p) cudaFree(b->p);
+  if (c->d_status) cudaFree(c->d_status);
+  if (c->d_queue) cudaFree(c->d_queue);
+  for (cudaEvent_t ev : {c->ev0, c->ev1, c->ev2, c->ev3, c->join[0], c->join[1]})
+    if (ev) cudaEventDestroy(ev);
+  for (int i = 0; i < 2; ++i)
+    if (c->copy[i]) cudaStreamDestroy(c->copy[i]);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return P2Z_OK;
+}
+
+p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
+                          const uint32_t *d_hit_mask, void *d_trk_out, void *stream, p2z_stats *stats) {
+  if (!ctx) return fail(nullptr, P2Z_BAD_ARG, "context is NULL");
+  Plan pl;
+  p2z_status r = make_plan(ctx, cfg, pl);
+  if (r != P2Z_OK) return r;
+  if (pl.nslots > 0 && (!d_trk_in || !d_hits || !d_trk_out)) return fail(ctx, P2Z_BAD_ARG, "NULL device buffer");
+  if (d_trk_in == d_trk_out && pl.nslots > 0) return fail(ctx, P2Z_BAD_ARG, "d_trk_out must not alias d_trk_in");
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const uint32_t *mask = d_hit_mask;
+  if (!mask && pl.uneven) {
+    r = internal_mask(ctx, pl, st, &mask);
+    if (r != P2Z_OK) return r;
+  }
+  RunArgs base;
+  std::memset(&base, 0, sizeof base);
+  base.trk = (const float *)d_trk_in;
+  base.hits = (const float *)d_hits;
+  base.out = (float *)d_trk_out;
+  base.mask = mask;
+  base.nlayer = pl.nlayer;
+  base.kfact = pl.kfact;
+  base.status = ctx->d_status;
+  const int schedule = resolve_schedule(pl, mask != nullptr);
+  int launches = 0;
+  if (stats) {
+    P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
+    P2Z_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+  }
+  for (int it = 0; it < pl.niter; ++it) {
+    r = enqueue_pass(ctx, pl, base, 0, pl.nslots, schedule, st, ctx->d_queue, &launches);
+    if (r != P2Z_OK) return r;
+  }
+  if (stats) {
+    P2Z_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+    P2Z_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    P2Z_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    unsigned int status = 0;
+    P2Z_CUDA(ctx, cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
+    std::memset(stats, 0, sizeof *stats);
+    stats->kernel_ms = ms;
+    stats->total_ms = ms;
+    stats->track_slots = pl.nslots;
+    r = count_updates(ctx, pl, mask, st, &stats->updates);
+    if (r != P2Z_OK) return r;
+    stats->launches = launches;
+    stats->singular = (status & 1u) ? 1 : 0;
+    if ((pl.flags & P2Z_FLAG_STRICT) && stats->singular)
+      return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
+  } else {
+    P2Z_CUDA(ctx, cudaGetLastError());
+  }
+  return P2Z_OK;
+}
+
+p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, const void *hits,
+                   const uint32_t *hit_mask, void *trk_out, p2z_stats *stats) {
+  if (!ctx) return fail(nullptr, P2Z_BAD_ARG, "context is NULL");
+  Plan pl;
+  p2z_status r = make_plan(ctx, cfg, pl);
+  if (r != P2Z_OK) return r;
+  if (pl.nslots > 0 && (!trk_in || !hits || !trk_out)) return fail(ctx, P2Z_BAD_ARG, "NULL host buffer");
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t tb = p2z_sizeof_mptrk(pl.B), hb = p2z_sizeof_mphit(pl.B);
+  const size_t trk_bytes = tb * (size_t)pl.nbatches;
+  const size_t hit_bytes = hb * (size_t)pl.nbatches * pl.nlayer;
+  if ((r = ensure(ctx, ctx->trk, trk_bytes)) != P2Z_OK) return r;
+  if ((r = ensure(ctx, ctx->hits, hit_bytes)) != P2Z_OK) return r;
+  if ((r = ensure(ctx, ctx->out, trk_bytes)) != P2Z_OK) return r;
+  const bool user_mask = hit_mask != nullptr;
+  const uint32_t *d_mask = nullptr;
+  if (user_mask) {
+    // ctx->mask is also the internal padding mask; a user mask replaces it.
+    if ((r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots)) != P2Z_OK) return r;
+    d_mask = (const uint32_t *)ctx->mask.p;
+  }
+  cudaStream_t s0 = ctx->copy[0], s1 = ctx->copy[1];
+  if (!user_mask && pl.uneven) {
+    r = internal_mask(ctx, pl, s0, &d_mask);
+    if (r != P2Z_OK) return r;
+    P2Z_CUDA(ctx, cudaEventRecord(ctx->join[0], s0));
+    P2Z_CUDA(ctx, cudaStreamWaitEvent(s1, ctx->join[0], 0));
+  }
+  RunArgs base;
+  std::memset(&base, 0, sizeof base);
+  base.trk = (const float *)ctx->trk.p;
+  base.hits = (const float *)ctx->hits.p;
+  base.out = (float *)ctx->out.p;
+  base.mask = d_mask;
+  base.nlayer = pl.nlayer;
+  base.kfact = pl.kfact;
+  base.status = ctx->d_status;
+  int schedule = resolve_schedule(pl, d_mask != nullptr);
+  // The per-event form is timed as it stands: copies first, then one launch per event.
+  const bool per_event = schedule == P2Z_SCHED_PER_EVENT;
+  // Only the 2-D updates read just the first 6 of the 9 hit words.
+  const bool six = (pl.upd == UPDK_V2 || pl.upd == UPDK_V2_COMP || pl.upd == UPDK_F64 || pl.upd == UPDK_V2_REF) &&
+                   !(pl.flags & P2Z_FLAG_FULL_HITS);
+  const int64_t nchunk = per_event ? 1 : std::max<int64_t>(1, std::min<int64_t>(8, pl.nbatches / 64));
+  const int64_t cb = nchunk ? (pl.nbatches + nchunk - 1) / nchunk : 0;
+  int launches = 0;
+  int64_t h2d = 0, d2h = 0;
+  P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), s0));
+  P2Z_CUDA(ctx, cudaEventRecord(ctx->ev0, s0));
+  P2Z_CUDA(ctx, cudaStreamWaitEvent(s1, ctx->ev0, 0));
+  for (int it = 0; it < pl.niter; ++it) {
+    for (int64_t c = 0; c < nchunk; ++c) {
+      cudaStream_t st = (c & 1) ? s1 : s0;
+      const int64_t b0 = c * cb, b1 = std::min(pl.nbatches, b0 + cb);
+      if (b1 <= b0) continue;
+      const int64_t nbc = b1 - b0;
+      P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->trk.p + b0 * tb, (const char *)trk_in + b0 * tb, nbc * tb,
+                                    cudaMemcpyHostToDevice, st));
+      h2d += nbc * tb;
+      const size_t hrow = hb, hrows = (size_t)nbc * pl.nlayer;
+      const size_t hoff = (size_t)b0 * pl.nlayer * hb;
+      if (six) {
+        const size_t w = 6 * (size_t)pl.B * 4;
+        P2Z_CUDA(ctx, cudaMemcpy2DAsync((char *)ctx->hits.p + hoff, hrow, (const char *)hits + hoff, hrow, w, hrows,
+                                        cudaMemcpyHostToDevice, st));
+        h2d += (int64_t)(w * hrows);
+      } else {
+        P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->hits.p + hoff, (const char *)hits + hoff, hrow * hrows,
+                                      cudaMemcpyHostToDevice, st));
+        h2d += (int64_t)(hrow * hrows);
+      }
+      if (user_mask) {
+        P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->mask.p + b0 * pl.B * 4, (const char *)hit_mask + b0 * pl.B * 4,
+                                      nbc * pl.B * 4, cudaMemcpyHostToDevice, st));
+        h2d += nbc * pl.B * 4;
+      }
+      if (!per_event) {
+        r = enqueue_pass(ctx, pl, base, b0 * pl.B, b1 * pl.B, schedule == P2Z_SCHED_PERSISTENT ? P2Z_SCHED_FLAT : schedule,
+                         st, ctx->d_queue + (c & 1), &launches);
+        if (r != P2Z_OK) return r;
+        P2Z_CUDA(ctx, cudaMemcpyAsync((char *)trk_out + b0 * tb, (const char *)ctx->out.p + b0 * tb, nbc * tb,
+                                      cudaMemcpyDeviceToHost, st));
+        d2h += nbc * tb;
+      }
+    }
+    if (per_event) {
+      r = enqueue_pass(ctx, pl, base, 0, pl.nslots, P2Z_SCHED_PER_EVENT, s0, ctx->d_queue, &launches);
+      if (r != P2Z_OK) return r;
+      P2Z_CUDA(ctx, cudaMemcpyAsync(trk_out, ctx->out.p, trk_bytes, cudaMemcpyDeviceToHost, s0));
+      d2h += trk_bytes;
+    }
+  }
+  P2Z_CUDA(ctx, cudaEventRecord(ctx->join[1], s1));
+  P2Z_CUDA(ctx, cudaStreamWaitEvent(s0, ctx->join[1], 0));
+  P2Z_CUDA(ctx, cudaEventRecord(ctx->ev1, s0));
+  P2Z_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  unsigned int status = 0;
+  P2Z_CUDA(ctx, cudaMemcpy(&status, ctx->d_status, sizeof status, cudaMemcpyDeviceToHost));
+  if (stats) {
+    float ms = 0.f;
+    P2Z_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    std::memset(stats, 0, sizeof *stats);
+    stats->total_ms = ms;
+    stats->track_slots = pl.nslots;
+    stats->h2d_bytes = h2d;
+    stats->d2h_bytes = d2h;
+    stats->launches = launches;
+    stats->singular = (status & 1u) ? 1 : 0;
+    r = count_updates(ctx, pl, d_mask, s0, &stats->updates);
+    if (r != P2Z_OK) return r;
+  }
+  if ((pl.flags & P2Z_FLAG_STRICT) && (status & 1u))
+    return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
+  return P2Z_OK;
+}
+
+p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *d_trk, const void *d_hits, int nlayer,
+                           int layer, int what, int update, float kfact) {
+  if (!ctx) return fail(nullptr, P2Z_BAD_ARG, "context is NULL");
+  if (!valid_bsize(bsize)) return fail(ctx, P2Z_UNSUPPORTED, "bsize %d not in {8,16,32,64}", bsize);
+  if (nbatches < 0 || nlayer < 1 || layer < 0 || layer >= nlayer || what < 1 || what > 3)
+    return fail(ctx, P2Z_BAD_ARG, "bad step arguments");
+  if (update != P2Z_UPDATE_V2) return fail(ctx, P2Z_UNSUPPORTED, "p2z_step_device implements the V2 update only");
+  if (nbatches > 0 && (!d_trk || !d_hits)) return fail(ctx, P2Z_BAD_ARG, "NULL device buffer");
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  const float kf = kfact != 0.f ? kfact : (float)(100. / (-0.299792458 * 3.8112));
+  P2Z_CUDA(ctx, launch_step(bsize, (float *)d_trk, (const float *)d_hits, nbatches * bsize, nlayer, layer, what, kf,
+                            ctx->stream));
+  P2Z_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return P2Z_OK;
+}
+
+p2z_status p2z_host_alloc(void **ptr, size_t bytes) {
+  if (!ptr) return fail(nullptr, P2Z_BAD_ARG, "ptr is NULL");
+  cudaError_t e = cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return fail(nullptr, e == cudaErrorMemoryAllocation ? P2Z_OOM : P2Z_CUDA_ERROR, "cudaHostAlloc(%zu): %s", bytes,
+                cudaGetErrorString(e));
+  }
+  return P2Z_OK;
+}
+
+p2z_status p2z_host_free(void *ptr) {
+  if (!ptr) return P2Z_OK;
+  cudaError_t e = cudaFreeHost(ptr);
+  if (e != cudaSuccess) return fail(nullptr, P2Z_CUDA_ERROR, "cudaFreeHost: %s", cudaGetErrorString(e));
+  return P2Z_OK;
+}
+
+}  // extern "C"

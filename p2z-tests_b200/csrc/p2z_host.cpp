@@ -1,0 +1,466 @@
+// p2z_host.cpp -- host-side pieces of the library: the reference-compatible
+// input preparation (prepareTracks / prepareHits), the physics workload
+// generator, layer masks for uneven workloads, and the validation block.
+// None of this is on the device hot path; it builds inputs and checks outputs
+// exactly as the reference's setup and reporting code does.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "p2z.h"
+
+namespace {
+
+constexpr int TRK_WORDS = 28;
+constexpr int HIT_WORDS = 9;
+
+bool valid_bsize(int b) { return b == 8 || b == 16 || b == 32 || b == 64; }
+
+// ---------------------------------------------------------------------------
+// Reference-compatible Gaussian stream
+// ---------------------------------------------------------------------------
+// The reference draws every smearing factor from randn (src/propagate-toz-
+// test_OMP.cpp:127-145): Marsaglia's polar method on the C library's rand(),
+// returning the two variates of an accepted pair on consecutive calls.  Types
+// follow the reference exactly: U = -1 + (float)rand()/RAND_MAX*2 in float,
+// W = pow(U1,2) + pow(U2,2) in double stored to float, mult = sqrtf(-2*logf(W)/W).
+// rand() after srand(1) is glibc's additive-feedback random(); random_r on a
+// private TYPE_3 state seeded with 1 yields the same sequence without touching
+// the process-wide generator.
+class RefGauss {
+ public:
+  RefGauss() {
+    std::memset(&rd_, 0, sizeof rd_);
+    std::memset(state_, 0, sizeof state_);
+    initstate_r(1u, state_, sizeof state_, &rd_);
+    srandom_r(1u, &rd_);
+  }
+  float next() {
+    if (have_second_) {
+      have_second_ = false;
+      return 0.f + 1.f * x2_;
+    }
+    float u1, u2, w;
+    do {
+      u1 = -1 + ((float)draw() / RAND_MAX) * 2;
+      u2 = -1 + ((float)draw() / RAND_MAX) * 2;
+      w = (float)((double)u1 * (double)u1 + (double)u2 * (double)u2);
+    } while (w >= 1 || w == 0);
+    const float mult = sqrtf((-2 * logf(w)) / w);
+    x1_ = u1 * mult;
+    x2_ = u2 * mult;
+    have_second_ = true;
+    return 0.f + 1.f * x1_;
+  }
+
+ private:
+  int32_t draw() {
+    int32_t r = 0;
+    random_r(&rd_, &r);
+    return r;
+  }
+  struct random_data rd_;
+  char state_[128];
+  float x1_ = 0.f, x2_ = 0.f;
+  bool have_second_ = false;
+};
+
+// The reference's smearing factor (1 + smear*randn), formed in double.  Its
+// builds compile with FMA contraction on (gcc -O3 -march=native), which turns
+// this expression into one fused multiply-add; that rounding is kept here.
+inline double smear_factor(double smear, float r) { return std::fma(smear, (double)r, 1.0); }
+
+// ---------------------------------------------------------------------------
+// Counter-based generator for the physics workload
+// ---------------------------------------------------------------------------
+// SplitMix64 (Steele, Lea, Flood 2014) finaliser applied to a per-track key
+// and a counter: the i-th draw of track t depends only on (seed, t, i).
+inline uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+struct TrackRng {
+  uint64_t key, ctr = 0;
+  TrackRng(uint64_t seed, uint64_t stream) : key(mix64(seed + 0x9E3779B97F4A7C15ull * (stream + 1))) {}
+  uint64_t bits() { return mix64(key + 0x9E3779B97F4A7C15ull * (++ctr)); }
+  double uniform() { return ((double)(bits() >> 11) + 0.5) * (1.0 / 9007199254740992.0); }  // (0,1)
+  double normal() {  // Box-Muller, one variate per call
+    const double u1 = uniform(), u2 = uniform();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  }
+};
+
+// Cholesky of a symmetric 6x6 (row-major); false if not positive definite.
+bool cholesky6(const double A[6][6], double L[6][6]) {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) L[i][j] = 0.0;
+  for (int j = 0; j < 6; ++j) {
+    double d = A[j][j];
+    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+    if (!(d > 1e-12)) return false;
+    L[j][j] = std::sqrt(d);
+    for (int i = j + 1; i < 6; ++i) {
+      double s = A[i][j];
+      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+      L[i][j] = s / L[j][j];
+    }
+  }
+  return true;
+}
+
+inline int sym(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
+int host_threads(int requested) {
+  if (requested > 0) return requested;
+  const unsigned h = std::thread::hardware_concurrency();
+  return h ? (int)h : 1;
+}
+
+template <class F>
+void parallel_for(int64_t n, int nthr, F f) {
+  nthr = (int)std::max<int64_t>(1, std::min<int64_t>(nthr, n));
+  if (nthr <= 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int64_t chunk = (n + nthr - 1) / nthr;
+  for (int t = 0; t < nthr; ++t) {
+    const int64_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a >= b) break;
+    th.emplace_back([=] { f(a, b); });
+  }
+  for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
+                       int64_t ntrks, int nlayer, double smear, double cov_scale, void *trk_out, void *hits_out) {
+  if (!seed || !hit_seeds || !trk_out || !hits_out) return P2Z_BAD_ARG;
+  if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize || nlayer < 1 || nlayer > 32) return P2Z_BAD_ARG;
+  if (nseeds < nlayer) return P2Z_BAD_ARG;  // the reference exits here (:271-274)
+  const int64_t nb = ntrks / bsize;
+  float *T = (float *)trk_out;
+  float *H = (float *)hits_out;
+  RefGauss g;
+  // prepareTracks (:243-263): event, batch, lane; 6 parameters then 21
+  // covariance elements, each scaled by (1 + smear*randn); cov also * cov_scale.
+  for (int64_t ie = 0; ie < nevts; ++ie)
+    for (int64_t ib = 0; ib < nb; ++ib) {
+      float *b = T + (ib + nb * ie) * (int64_t)TRK_WORDS * bsize;
+      for (int it = 0; it < bsize; ++it) {
+        for (int ip = 0; ip < 6; ++ip) b[it + ip * bsize] = smear_factor(smear, g.next()) * seed->par[ip];
+        for (int ip = 0; ip < 21; ++ip)
+          b[6 * bsize + it + ip * bsize] = smear_factor(smear, g.next()) * seed->cov[ip] * cov_scale;
+        std::memcpy(&b[27 * bsize + it], &seed->q, sizeof(int32_t));
+      }
+    }
+  // prepareHits (:265-293): layer outermost; layer l of batch ib of event ie
+  // at hit batch l + nlayer*(ib + nb*ie).
+  for (int lay = 0; lay < nlayer; ++lay) {
+    const p2z_ahit &s = hit_seeds[lay];
+    for (int64_t ie = 0; ie < nevts; ++ie)
+      for (int64_t ib = 0; ib < nb; ++ib) {
+        float *h = H + (lay + nlayer * (ib + nb * ie)) * (int64_t)HIT_WORDS * bsize;
+        for (int it = 0; it < bsize; ++it) {
+          for (int ip = 0; ip < 3; ++ip) h[it + ip * bsize] = smear_factor(smear, g.next()) * s.pos[ip];
+          for (int ip = 0; ip < 6; ++ip) h[3 * bsize + it + ip * bsize] = smear_factor(smear, g.next()) * s.cov[ip];
+        }
+      }
+  }
+  return P2Z_OK;
+}
+
+void p2z_physics_defaults(p2z_physics_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->seed = 20240601ull;
+  p->pt_min = 0.5;
+  p->pt_max = 20.0;
+  p->eta_min = 1.6;
+  p->eta_max = 2.5;
+  p->sigma_vz = 5.0;
+  p->sig_xy = 0.01;
+  p->sig_z = 0.05;
+  p->rel_sig_ipt = 0.01;
+  p->sig_phi = 1e-3;
+  p->sig_theta = 1e-3;
+  p->rho_max = 0.3;
+  p->z_first = 30.0;
+  p->z_last = 270.0;
+  p->hit_sig_xy = 30e-4;  // 30 um in cm
+  p->hit_sig_z = 1e-4;    // 1 um in cm
+  p->kfact = 0.f;
+  p->nthreads = 0;
+}
+
+p2z_status p2z_generate_physics(const p2z_physics_params *p, const p2z_config *cfg, void *trk_out, void *hits_out,
+                                uint32_t *hit_mask) {
+  if (!p || !cfg || !trk_out || !hits_out) return P2Z_BAD_ARG;
+  if (!valid_bsize(cfg->bsize)) return P2Z_UNSUPPORTED;
+  const int B = cfg->bsize, nlayer = cfg->nlayer;
+  if (nlayer < 1 || nlayer > 32 || cfg->nevts < 0) return P2Z_BAD_ARG;
+  if (p->pt_min <= 0 || p->pt_max < p->pt_min || p->eta_max < p->eta_min) return P2Z_BAD_ARG;
+  // event -> [first slot, number of real tracks)
+  std::vector<int64_t> ev_first(cfg->nevts), ev_n(cfg->nevts);
+  int64_t nb = 0;
+  for (int64_t e = 0; e < cfg->nevts; ++e) {
+    const int64_t n = cfg->event_ntrks ? cfg->event_ntrks[e] : cfg->ntrks;
+    if (n < 0 || (!cfg->event_ntrks && n % B)) return P2Z_BAD_ARG;
+    ev_first[e] = nb * B;
+    ev_n[e] = n;
+    nb += (n + B - 1) / B;
+  }
+  const int64_t nslots = nb * B;
+  // slot -> event lookup through the batch's event
+  std::vector<int64_t> batch_event(nb);
+  for (int64_t e = 0; e < cfg->nevts; ++e) {
+    const int64_t b0 = ev_first[e] / B, nbe = (ev_n[e] + B - 1) / B;
+    for (int64_t i = 0; i < nbe; ++i) batch_event[b0 + i] = e;
+  }
+  const double kf = p->kfact != 0.f ? p->kfact : (double)(float)(100. / (-0.299792458 * 3.8112));
+  const uint32_t all = nlayer >= 32 ? 0xffffffffu : ((1u << nlayer) - 1u);
+  float *T = (float *)trk_out;
+  float *H = (float *)hits_out;
+  const double lpt0 = std::log(p->pt_min), lpt1 = std::log(p->pt_max);
+  parallel_for(nslots, host_threads(p->nthreads), [&](int64_t s0, int64_t s1) {
+    for (int64_t s = s0; s < s1; ++s) {
+      const int64_t b = s / B;
+      const int t = (int)(s % B);
+      float *tb = T + b * (int64_t)TRK_WORDS * B;
+      const int64_t e = batch_event[b];
+      const bool real = (s - ev_first[e]) < ev_n[e];
+      if (!real) {
+        for (int w = 0; w < TRK_WORDS; ++w) tb[t + w * B] = 0.f;
+        for (int l = 0; l < nlayer; ++l) {
+          float *hb = H + (b * nlayer + l) * (int64_t)HIT_WORDS * B;
+          for (int w = 0; w < HIT_WORDS; ++w) hb[t + w * B] = 0.f;
+        }
+        if (hit_mask) hit_mask[s] = 0u;
+        continue;
+      }
+      TrackRng r(p->seed, (uint64_t)s);
+      const int q = r.uniform() < 0.5 ? -1 : 1;
+      const double pt = std::exp(lpt0 + (lpt1 - lpt0) * r.uniform());
+      const double ipt = 1.0 / pt;
+      const double phi = -M_PI + 2.0 * M_PI * r.uniform();
+      const double eta = p->eta_min + (p->eta_max - p->eta_min) * r.uniform();
+      const double theta = 2.0 * std::atan(std::exp(-eta));
+      const double vz = p->sigma_vz * r.normal();
+      const double truth[6] = {0.0, 0.0, vz, ipt, phi, theta};
+      const double sig[6] = {p->sig_xy, p->sig_xy, p->sig_z, p->rel_sig_ipt * ipt, p->sig_phi, p->sig_theta};
+      // random correlation, |rho| <= rho_max, positive definite
+      double rho[6][6], L[6][6];
+      bool ok = false;
+      for (int attempt = 0; attempt < 64 && !ok; ++attempt) {
+        const double shrink = attempt < 32 ? 1.0 : std::pow(0.5, attempt - 31);
+        for (int i = 0; i < 6; ++i) {
+          rho[i][i] = 1.0;
+          for (int j = 0; j < i; ++j) rho[i][j] = rho[j][i] = shrink * p->rho_max * (2.0 * r.uniform() - 1.0);
+        }
+        ok = cholesky6(rho, L);
+      }
+      if (!ok) {
+        for (int i = 0; i < 6; ++i)
+          for (int j = 0; j < 6; ++j) rho[i][j] = i == j ? 1.0 : 0.0;
+        cholesky6(rho, L);
+      }
+      // initial state = truth + D L n
+      double n6[6];
+      for (int i = 0; i < 6; ++i) n6[i] = r.normal();
+      double par[6];
+      for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+        for (int k = 0; k <= i; ++k) acc += L[i][k] * n6[k];
+        par[i] = truth[i] + sig[i] * acc;
+      }
+      for (int i = 0; i < 6; ++i) tb[t + i * B] = (float)par[i];
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j <= i; ++j) tb[t + (6 + sym(i, j)) * B] = (float)(sig[i] * rho[i][j] * sig[j]);
+      std::memcpy(&tb[t + 27 * B], &q, sizeof q);
+      // hits on the planes, at the true helix point plus noise
+      const double k = q * kf;
+      const double cP = std::cos(phi), sP = std::sin(phi);
+      const double tanT = std::tan(theta);
+      for (int l = 0; l < nlayer; ++l) {
+        const double zl = nlayer > 1 ? p->z_first + (p->z_last - p->z_first) * l / (nlayer - 1) : p->z_first;
+        const double alpha = (zl - vz) * tanT * ipt / k;
+        const double sa = std::sin(alpha), ca = std::cos(alpha);
+        const double hx = truth[0] + k * pt * (cP * sa - sP * (1.0 - ca));
+        const double hy = truth[1] + k * pt * (sP * sa + cP * (1.0 - ca));
+        float *hb = H + (b * nlayer + l) * (int64_t)HIT_WORDS * B;
+        hb[t + 0 * B] = (float)(hx + p->hit_sig_xy * r.normal());
+        hb[t + 1 * B] = (float)(hy + p->hit_sig_xy * r.normal());
+        hb[t + 2 * B] = (float)(zl + p->hit_sig_z * r.normal());
+        const float vxy = (float)(p->hit_sig_xy * p->hit_sig_xy), vz2 = (float)(p->hit_sig_z * p->hit_sig_z);
+        hb[t + 3 * B] = vxy;
+        hb[t + 4 * B] = 0.f;
+        hb[t + 5 * B] = vxy;
+        hb[t + 6 * B] = 0.f;
+        hb[t + 7 * B] = 0.f;
+        hb[t + 8 * B] = vz2;
+      }
+      if (hit_mask) hit_mask[s] = all;
+    }
+  });
+  return P2Z_OK;
+}
+
+p2z_status p2z_mask_layers(uint32_t *hit_mask, int64_t nslots, int nlayer, int min_hits, int max_hits,
+                           double drop_prob, uint64_t seed) {
+  if (!hit_mask && nslots > 0) return P2Z_BAD_ARG;
+  if (nlayer < 1 || nlayer > 32 || min_hits < 1 || max_hits < min_hits || max_hits > nlayer || drop_prob < 0 ||
+      drop_prob >= 1)
+    return P2Z_BAD_ARG;
+  parallel_for(nslots, host_threads(0), [&](int64_t s0, int64_t s1) {
+    for (int64_t s = s0; s < s1; ++s) {
+      if (hit_mask[s] == 0u) continue;
+      TrackRng r(seed ^ 0x5bd1e995ull, (uint64_t)s);
+      const int L = min_hits + (int)std::min<double>(max_hits - min_hits, std::floor(r.uniform() * (max_hits - min_hits + 1)));
+      uint32_t m = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+      int count = L;
+      for (int l = 0; l < L; ++l) {
+        if (count > min_hits && r.uniform() < drop_prob) {
+          m &= ~(1u << l);
+          --count;
+        }
+      }
+      hit_mask[s] = m;
+    }
+  });
+  return P2Z_OK;
+}
+
+p2z_status p2z_validate(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
+                        p2z_validation *v) {
+  if (!trk_out || !hit_last || !v) return P2Z_BAD_ARG;
+  if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize) return P2Z_BAD_ARG;
+  const float *T = (const float *)trk_out;
+  const int64_t nb = ntrks / bsize;
+  auto get = [&](int64_t ie, int64_t it, int p) -> float {
+    const int64_t ib = it / bsize;
+    const int lane = (int)(it % bsize);
+    return T[(ib + nb * ie) * (int64_t)TRK_WORDS * bsize + lane + p * bsize];
+  };
+  const double hx_ = hit_last[0], hy_ = hit_last[1], hz_ = hit_last[2];
+  // The reference's two passes (src/propagate-toz-test_OMP.cpp:758-864):
+  // skip non-finite tracks, skip tracks outside its fixed window, then
+  // accumulate means and spreads in double over the rest.
+  auto finite6 = [](double a, double b, double c, double d, double e, double f) {
+    return std::isfinite(a) && std::isfinite(b) && std::isfinite(c) && std::isfinite(d) && std::isfinite(e) &&
+           std::isfinite(f);
+  };
+  auto outside = [&](double x_, double y_, double z_, double pt_, double phi_, double theta_) {
+    return std::fabs((x_ - hx_) / hx_) > 1. || std::fabs((y_ - hy_) / hy_) > 1. || std::fabs((z_ - hz_) / hz_) > 1. ||
+           std::fabs((pt_ - 12.) / 12.) > 1. || std::fabs((phi_ - 1.3) / 1.3) > 1. ||
+           std::fabs((theta_ - 2.8) / 2.8) > 1.;
+  };
+  int64_t nnans = 0, nfail = 0, ngood = 0;
+  double avgx = 0, avgy = 0, avgz = 0, avgpt = 0, avgphi = 0, avgtheta = 0, avgdx = 0, avgdy = 0, avgdz = 0;
+  for (int64_t ie = 0; ie < nevts; ++ie)
+    for (int64_t it = 0; it < ntrks; ++it) {
+      const double x_ = get(ie, it, 0), y_ = get(ie, it, 1), z_ = get(ie, it, 2);
+      const double pt_ = 1. / get(ie, it, 3), phi_ = get(ie, it, 4), theta_ = get(ie, it, 5);
+      if (!finite6(x_, y_, z_, pt_, phi_, theta_)) {
+        nnans++;
+        continue;
+      }
+      if (outside(x_, y_, z_, pt_, phi_, theta_)) {
+        nfail++;
+        continue;
+      }
+      avgpt += pt_;
+      avgphi += phi_;
+      avgtheta += theta_;
+      avgx += x_;
+      avgy += y_;
+      avgz += z_;
+      avgdx += (x_ - hx_) / x_;
+      avgdy += (y_ - hy_) / y_;
+      avgdz += (z_ - hz_) / z_;
+      ngood++;
+    }
+  avgpt /= double(ngood);
+  avgphi /= double(ngood);
+  avgtheta /= double(ngood);
+  avgx /= double(ngood);
+  avgy /= double(ngood);
+  avgz /= double(ngood);
+  avgdx /= double(ngood);
+  avgdy /= double(ngood);
+  avgdz /= double(ngood);
+  double stdx = 0, stdy = 0, stdz = 0, stddx = 0, stddy = 0, stddz = 0;
+  for (int64_t ie = 0; ie < nevts; ++ie)
+    for (int64_t it = 0; it < ntrks; ++it) {
+      const double x_ = get(ie, it, 0), y_ = get(ie, it, 1), z_ = get(ie, it, 2);
+      const double pt_ = 1. / get(ie, it, 3), phi_ = get(ie, it, 4), theta_ = get(ie, it, 5);
+      if (!finite6(x_, y_, z_, pt_, phi_, theta_)) continue;
+      if (outside(x_, y_, z_, pt_, phi_, theta_)) continue;
+      stdx += (x_ - avgx) * (x_ - avgx);
+      stdy += (y_ - avgy) * (y_ - avgy);
+      stdz += (z_ - avgz) * (z_ - avgz);
+      stddx += ((x_ - hx_) / x_ - avgdx) * ((x_ - hx_) / x_ - avgdx);
+      stddy += ((y_ - hy_) / y_ - avgdy) * ((y_ - hy_) / y_ - avgdy);
+      stddz += ((z_ - hz_) / z_ - avgdz) * ((z_ - hz_) / z_ - avgdz);
+    }
+  // The reference takes these roots with sqrtf, i.e. in single precision.
+  v->stdx = sqrtf((float)(stdx / double(ngood)));
+  v->stdy = sqrtf((float)(stdy / double(ngood)));
+  v->stdz = sqrtf((float)(stdz / double(ngood)));
+  v->stddx = sqrtf((float)(stddx / double(ngood)));
+  v->stddy = sqrtf((float)(stddy / double(ngood)));
+  v->stddz = sqrtf((float)(stddz / double(ngood)));
+  v->avgx = avgx;
+  v->avgy = avgy;
+  v->avgz = avgz;
+  v->avgdx = avgdx;
+  v->avgdy = avgdy;
+  v->avgdz = avgdz;
+  v->avgpt = avgpt;
+  v->avgphi = avgphi;
+  v->avgtheta = avgtheta;
+  v->nnans = nnans;
+  v->nfail = nfail;
+  v->ngood = ngood;
+  return P2Z_OK;
+}
+
+void p2z_print_validation(const p2z_validation *v) {
+  if (!v) return;
+  // Text of the reference's block, line for line (:866-876).
+  std::printf("track x avg=%f std/avg=%f\n", v->avgx, std::fabs(v->stdx / v->avgx));
+  std::printf("track y avg=%f std/avg=%f\n", v->avgy, std::fabs(v->stdy / v->avgy));
+  std::printf("track z avg=%f std/avg=%f\n", v->avgz, std::fabs(v->stdz / v->avgz));
+  std::printf("track dx/x avg=%f std=%f\n", v->avgdx, v->stddx);
+  std::printf("track dy/y avg=%f std=%f\n", v->avgdy, v->stddy);
+  std::printf("track dz/z avg=%f std=%f\n", v->avgdz, v->stddz);
+  std::printf("track pt avg=%f\n", v->avgpt);
+  std::printf("track phi avg=%f\n", v->avgphi);
+  std::printf("track theta avg=%f\n", v->avgtheta);
+  std::printf("number of tracks with nans=%i\n", (int)v->nnans);
+  std::printf("number of tracks failed=%i\n", (int)v->nfail);
+  std::fflush(stdout);
+}
+
+void p2z_print_formatted(int niter, int64_t nevts, int64_t ntrks, int bsize, double wall_s, double setup_s,
+                         int nthreads) {
+  // The reference's machine-readable line (:756), read positionally by its
+  // tools (tools/compare.py:12).
+  std::printf("formatted %i %i %i %i %i %f 0 %f %i\n", niter, (int)nevts, (int)ntrks, bsize,
+              bsize ? (int)(ntrks / bsize) : 0, wall_s, setup_s, nthreads);
+  std::fflush(stdout);
+}
+
+}  // extern "C"

@@ -1,0 +1,307 @@
+// p2z_kernels.cuh -- hot-path kernels (templates; instantiated per update kind
+// in p2z_kern_*.cu).
+//
+// One thread owns one track slot (batch b, lane t of a bsize-wide AOSOA batch)
+// and keeps the track's parameters and live covariance in registers across all
+// its layers: the reference's per-layer loop (src/propagate-toz-test_OMP.cpp:
+// 740-745, GPU form src/propagate-toz-test_CUDA_v4.cu:761-775) runs entirely on
+// registers and the only memory traffic is one read of the track, one read of
+// the 6 (v2) or 9 (3x3) hit words per present layer and one write of the track.
+//
+// Loads of the AOSOA arrays are coalesced: for a fixed element, consecutive
+// lanes read consecutive words (a 32-lane warp reads 128 contiguous bytes when
+// bsize >= 32, or 32-byte sector runs of bsize*4 bytes otherwise).  The hits of
+// the next present layer are requested before the current layer is computed,
+// so their latency overlaps the arithmetic.
+#pragma once
+
+#include <type_traits>
+
+#include "p2z_math.cuh"
+
+namespace p2z {
+
+constexpr int TRK_WORDS = 28;  // 6 par + 21 cov + 1 q
+constexpr int HIT_WORDS = 9;   // 3 pos + 6 cov
+
+// Kernel kinds
+enum { KIND_FLAT = 0, KIND_PERSISTENT = 1 };
+// Arithmetic of a kernel instance:
+//  UPDK_V2       precise FP32 form, FP64 x/y/phi accumulators, the reference's 2-D update
+//  UPDK_V2_COMP  precise FP32 form with no FP64 at all: float-pair accumulators,
+//                compensated 2x2 determinant
+//  UPDK_3X3_F64  precise FP32 propagation; 3x3 inversion + Joseph update in FP64
+//  UPDK_3X3_COMP precise FP32 propagation; 3x3 + Joseph in FP32 with compensated
+//                cofactors, float-pair accumulators (FP64-free)
+//  UPDK_F64      everything in FP64
+//  UPDK_V2_REF   the reference's own FP32 evaluation (FORM_REFERENCE); its
+//                translation unit is compiled without FMA contraction
+enum { UPDK_V2 = 0, UPDK_V2_COMP = 1, UPDK_3X3_F64 = 2, UPDK_3X3_COMP = 3, UPDK_F64 = 4, UPDK_V2_REF = 5 };
+
+template <int UPD>
+struct Types {
+  using T = typename std::conditional<UPD == UPDK_F64, double, float>::type;
+  using A = typename std::conditional<
+      UPD == UPDK_F64, double,
+      typename std::conditional<UPD == UPDK_V2_REF, float,
+                                typename std::conditional<UPD == UPDK_V2_COMP || UPD == UPDK_3X3_COMP, DF,
+                                                          double>::type>::type>::type;
+  static constexpr int NH = (UPD == UPDK_3X3_F64 || UPD == UPDK_3X3_COMP) ? 9 : 6;
+};
+
+struct RunArgs {
+  const float *__restrict__ trk;   // MPTRK[nbatches]
+  const float *__restrict__ hits;  // MPHIT[nlayer * nbatches]
+  float *__restrict__ out;         // MPTRK[nbatches]
+  const uint32_t *__restrict__ mask;  // one word per slot, or null (all layers)
+  int64_t slot_begin, slot_end;    // slots [begin, end) of this launch
+  int nlayer;
+  float kfact;
+  unsigned int *status;            // bit 0: a det <= 0 was met
+  unsigned long long *queue;       // persistent kernels: next work item
+};
+
+template <int B>
+__device__ __forceinline__ const float *trk_lane(const float *base, int64_t slot) {
+  const int64_t b = slot / B;
+  const int t = (int)(slot % B);
+  return base + b * (int64_t)(TRK_WORDS * B) + t;
+}
+
+// Hit words of slot's batch on layer l: &pos.data[t], stride B per element.
+template <int B>
+__device__ __forceinline__ const float *hit_lane(const float *hits, int64_t slot, int nlayer, int l) {
+  const int64_t b = slot / B;
+  const int t = (int)(slot % B);
+  return hits + (b * nlayer + l) * (int64_t)(HIT_WORDS * B) + t;
+}
+
+// Hit words a kernel needs: x, y, z, V00, V10, V11 and, for the 3-D update,
+// V20, V21, V22.
+template <int NH>
+struct HitRegs {
+  float w[NH];
+};
+
+template <int B, int NH>
+__device__ __forceinline__ void load_hit(HitRegs<NH> &h, const float *p) {
+  // pos[0..2] then cov[0..NH-4]; element e of the lane at p[e*B]
+#pragma unroll
+  for (int e = 0; e < NH; ++e) h.w[e] = __ldg(p + e * B);
+}
+
+// One propagate + update step.  GENERAL: first present layer (full 21-element
+// input covariance in b21).  Returns true if the update met det <= 0.
+template <int UPD, int SC, bool GENERAL>
+__device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<UPD>::A> &s,
+                                     const typename Types<UPD>::T (&b21)[21], const HitRegs<Types<UPD>::NH> &h,
+                                     typename Types<UPD>::T k, typename Types<UPD>::T ik) {
+  using T = typename Types<UPD>::T;
+  const T zout = T(h.w[2]);
+  Helix<T> hx;
+  Jac<T> J;
+  if constexpr (UPD == UPDK_F64) {
+    hx = propagate_params_f64(s, zout, k);
+    J = jacobian_precise<double>(hx, k, s.ipt);
+  } else if constexpr (UPD == UPDK_V2_REF) {
+    hx = propagate_params_ref(s, zout, k);
+    J = jacobian_ref(hx, k, s.ipt);
+  } else {
+    hx = propagate_params_precise<SC>(s, zout, k, ik);
+    J = jacobian_precise<float>(hx, k, s.ipt);
+  }
+  if constexpr (GENERAL) propagate_cov_general(s, b21, hx, J);
+  else propagate_cov_reduced(s, J);
+  if constexpr (UPD == UPDK_F64) {
+    const double hp[3] = {h.w[0], h.w[1], h.w[2]};
+    const double hc[3] = {h.w[3], h.w[4], h.w[5]};
+    return update_v2_f64(s, hp, hc);
+  } else {
+    const float hp[3] = {h.w[0], h.w[1], h.w[2]};
+    if constexpr (UPD == UPDK_V2 || UPD == UPDK_V2_REF) {
+      const float hc[3] = {h.w[3], h.w[4], h.w[5]};
+      return update_v2<typename Types<UPD>::A, (UPD == UPDK_V2_REF) ? FORM_REFERENCE : FORM_PRECISE>(s, hp, hc);
+    } else if constexpr (UPD == UPDK_V2_COMP) {
+      const float hc[3] = {h.w[3], h.w[4], h.w[5]};
+      return update_v2_comp(s, hp, hc);
+    } else {
+      const float hv[6] = {h.w[3], h.w[4], h.w[5], h.w[6], h.w[7], h.w[8]};
+      if constexpr (UPD == UPDK_3X3_F64) return update_3x3_joseph<double>(s, hp, hv);
+      else return update_3x3_joseph<float>(s, hp, hv);
+    }
+  }
+}
+
+// Process one track slot: load, run every present layer, store.
+template <int B, int UPD, int SC, bool MASKED>
+__device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
+  using T = typename Types<UPD>::T;
+  using A = typename Types<UPD>::A;
+  constexpr int NH = Types<UPD>::NH;
+  const float *tin = trk_lane<B>(a.trk, slot);
+  float *tout = const_cast<float *>(trk_lane<B>(a.out, slot));
+
+  const uint32_t all = (a.nlayer >= 32) ? 0xffffffffu : ((1u << a.nlayer) - 1u);
+  uint32_t m = MASKED ? (__ldg(a.mask + slot) & all) : all;
+
+  float in[TRK_WORDS];
+#pragma unroll
+  for (int e = 0; e < TRK_WORDS; ++e) in[e] = __ldg(tin + e * B);
+
+  if (m == 0u) {  // no hits (or a padding slot): the track passes through
+#pragma unroll
+    for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, in[e]);
+    return;
+  }
+
+  const int q = __float_as_int(in[27]);
+  const float kf = float(q) * a.kfact;  // reference: q*kfact in float (:627)
+  const T k = T(kf);
+  const T ik = T(1) / k;
+
+  Trk<T, A> s;
+  acc_set(s.x, in[0]);
+  acc_set(s.y, in[1]);
+  acc_set(s.phi, in[4]);
+  s.z = in[2]; s.ipt = in[3]; s.theta = in[5];
+  T b21[21];
+#pragma unroll
+  for (int e = 0; e < 21; ++e) b21[e] = T(in[6 + e]);
+
+  bool singular = false;
+  const int l = __ffs(m) - 1;
+  uint32_t rest = m & (m - 1u);
+  HitRegs<NH> h, hn;
+  load_hit<B, NH>(h, hit_lane<B>(a.hits, slot, a.nlayer, l));
+  if (rest) load_hit<B, NH>(hn, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+  singular |= step<UPD, SC, true>(s, b21, h, k, ik);
+
+  while (rest) {
+    h = hn;
+    rest &= rest - 1u;
+    if (rest) load_hit<B, NH>(hn, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+    singular |= step<UPD, SC, false>(s, b21, h, k, ik);
+  }
+
+  const float z0 = 0.0f;
+  float o[TRK_WORDS];
+  o[0] = tof(s.x); o[1] = tof(s.y); o[2] = float(s.z);
+  o[3] = float(s.ipt); o[4] = tof(s.phi); o[5] = float(s.theta);
+  float *c = o + 6;
+  c[0] = float(s.c00); c[1] = float(s.c10); c[2] = float(s.c11);
+  c[3] = z0; c[4] = z0; c[5] = z0;
+  c[6] = float(s.c30); c[7] = float(s.c31); c[8] = z0; c[9] = float(s.c33);
+  c[10] = float(s.c40); c[11] = float(s.c41); c[12] = z0; c[13] = float(s.c43); c[14] = float(s.c44);
+  c[15] = float(s.c50); c[16] = float(s.c51); c[17] = z0; c[18] = float(s.c53); c[19] = float(s.c54);
+  c[20] = float(s.c55);
+  o[27] = in[27];
+#pragma unroll
+  for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, o[e]);
+  if (singular) atomicOr(a.status, 1u);
+}
+
+// One launch over slots [slot_begin, slot_end), one thread per slot.
+template <int B, int UPD, int SC, bool MASKED>
+__global__ void __launch_bounds__(256) k_flat(RunArgs a) {
+  const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= a.slot_end) return;
+  process_slot<B, UPD, SC, MASKED>(a, slot);
+}
+
+// Persistent launch: grid = resident CTAs; each warp repeatedly takes the next
+// 32-slot work item from a device counter (reset to 0 before the launch) until
+// the range is exhausted.  Work items are taken in slot order, so concurrently
+// running warps read neighbouring batches.
+template <int B, int UPD, int SC, bool MASKED>
+__global__ void __launch_bounds__(256) k_persistent(RunArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nslots = a.slot_end - a.slot_begin;
+  const unsigned long long nitems = (unsigned long long)((nslots + 31) / 32);
+  for (;;) {
+    unsigned long long item = 0;
+    if (lane == 0) item = atomicAdd(a.queue, 1ull);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int64_t slot = a.slot_begin + (int64_t)item * 32 + lane;
+    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, slot);
+  }
+}
+
+// Launch description used by the dispatch functions.
+struct LaunchSpec {
+  RunArgs args;
+  int bsize;
+  int upd;       // UPDK_*
+  int sc;        // SC_*
+  bool masked;
+  int kind;      // KIND_*
+  int block;     // threads per CTA
+  int grid;      // CTAs (persistent); flat computes its own
+};
+
+// Per-update-kind dispatchers (one translation unit each).
+cudaError_t launch_v2(const LaunchSpec &s, cudaStream_t st);
+cudaError_t launch_v2_comp(const LaunchSpec &s, cudaStream_t st);
+cudaError_t launch_3x3_f64(const LaunchSpec &s, cudaStream_t st);
+cudaError_t launch_3x3_comp(const LaunchSpec &s, cudaStream_t st);
+cudaError_t launch_f64(const LaunchSpec &s, cudaStream_t st);
+cudaError_t launch_v2_ref(const LaunchSpec &s, cudaStream_t st);
+// Occupancy (resident CTAs per SM) of the kernel a spec selects.
+int occupancy_v2(const LaunchSpec &s);
+int occupancy_v2_comp(const LaunchSpec &s);
+int occupancy_3x3_f64(const LaunchSpec &s);
+int occupancy_3x3_comp(const LaunchSpec &s);
+int occupancy_f64(const LaunchSpec &s);
+int occupancy_v2_ref(const LaunchSpec &s);
+
+// Shared dispatch body: picks the template instance for (B, SC, MASKED, KIND).
+template <int UPD, bool HAS_FAST>
+struct Dispatch {
+  template <int B, int SC, bool M>
+  static const void *fn(int kind) {
+    return kind == KIND_PERSISTENT ? (const void *)k_persistent<B, UPD, SC, M> : (const void *)k_flat<B, UPD, SC, M>;
+  }
+  template <int B, int SC>
+  static const void *fn_m(bool masked, int kind) {
+    return masked ? fn<B, SC, true>(kind) : fn<B, SC, false>(kind);
+  }
+  template <int B>
+  static const void *fn_sc(int sc, bool masked, int kind) {
+    if constexpr (HAS_FAST) {
+      if (sc == SC_FAST) return fn_m<B, SC_FAST>(masked, kind);
+    }
+    return fn_m<B, SC_ACCURATE>(masked, kind);
+  }
+  static const void *select(const LaunchSpec &s) {
+    switch (s.bsize) {
+      case 8: return fn_sc<8>(s.sc, s.masked, s.kind);
+      case 16: return fn_sc<16>(s.sc, s.masked, s.kind);
+      case 32: return fn_sc<32>(s.sc, s.masked, s.kind);
+      case 64: return fn_sc<64>(s.sc, s.masked, s.kind);
+      default: return nullptr;
+    }
+  }
+  static cudaError_t launch(const LaunchSpec &s, cudaStream_t st) {
+    const void *f = select(s);
+    if (!f) return cudaErrorInvalidValue;
+    const int64_t n = s.args.slot_end - s.args.slot_begin;
+    if (n <= 0) return cudaSuccess;
+    int grid;
+    if (s.kind == KIND_PERSISTENT) {
+      grid = s.grid;
+    } else {
+      grid = (int)((n + s.block - 1) / s.block);
+    }
+    RunArgs a = s.args;
+    void *params[] = {&a};
+    return cudaLaunchKernel(f, dim3(grid), dim3(s.block), params, 0, st);
+  }
+  static int occupancy(const LaunchSpec &s) {
+    const void *f = select(s);
+    int nb = 0;
+    if (!f || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, s.block, 0) != cudaSuccess) return 0;
+    return nb;
+  }
+};
+
+}  // namespace p2z

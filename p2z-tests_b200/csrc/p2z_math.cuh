@@ -1,0 +1,550 @@
+// p2z_math.cuh -- per-track device arithmetic of the propagate-to-z + Kalman
+// update hot path.
+//
+// Each function works on one track held in registers.  The algebra is the
+// reference's propagateToZ (src/propagate-toz-test_OMP.cpp:623-682) with its two
+// covariance products MultHelixPropEndcap (:296-341) and
+// MultHelixPropTranspEndcap (:343-373), followed by KalmanUpdate_v2 (:503-620).
+//
+// Two evaluation forms of that algebra are provided:
+//
+// FORM_PRECISE (the default): FP32 bulk arithmetic, evaluated so that it agrees
+//   with an all-FP64 evaluation to ~1e-6 in the parameters.  Two changes from
+//   the reference's FP32 evaluation, both exact in real arithmetic:
+//   * 1 - cos(a), for the helix angle a = alpha and for a = cosP*sin(alpha),
+//     is computed as the versine directly (a Taylor series of
+//     a^2/2 - a^4/24 + ..., or 2 sin^2(a/2)) instead of subtracting a rounded
+//     cosine from 1.  For high-pT tracks R*(1 - cos alpha) is the curvature
+//     (sagitta) signal and the subtraction in FP32 loses most of its digits,
+//     which the reference's FP32 build turns into ~1e-4 relative error in q/pT
+//     and ~1e-3 in the covariance.
+//   * x, y and phi are carried as accumulators wider than FP32 (FP64, or a
+//     float pair in the FP64-free variant): positions of tens of cm held in
+//     FP32 round at ~4e-6 cm, which against 30 um hits biases the curvature.
+// FORM_REFERENCE: the reference's FP32 evaluation operation for operation,
+//   including its C type promotions (the double literals in `1./ipt`,
+//   `1.0/cosT`, `(1.-cosa)` ... and the double determinant), for callers who
+//   want the reference's own rounding.  Compiled without FMA contraction and
+//   with correctly rounded sin/cos, it reproduces the reference built with
+//   -ffp-contract=off.
+//
+// Structure exploited (exact for finite inputs, both forms):
+//  * The Endcap products zero row and column 2 (z) of the propagated
+//    covariance, so after the first propagation only 15 of 21 covariance
+//    elements are live; every product with a z entry is a product with +-0.
+//  * The update after a propagation then has a zero z row in its gain: z stays
+//    at the hit's z and the z row/column stays zero.
+// The first present layer of a track therefore runs the general propagation
+// on the full 21-element input covariance; later layers run the reduced form.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace p2z {
+
+enum { SC_ACCURATE = 0, SC_FAST = 1 };
+enum { FORM_PRECISE = 0, FORM_REFERENCE = 1 };
+
+// ---------------------------------------------------------------------------
+// Accumulators for x, y, phi
+// ---------------------------------------------------------------------------
+// A float pair (hi + lo) with error-free additions (Knuth's TwoSum followed by
+// a Fast2Sum renormalisation) -- the FP64-free wide accumulator.
+struct DF {
+  float hi, lo;
+};
+
+__device__ __forceinline__ float tof(float v) { return v; }
+__device__ __forceinline__ float tof(double v) { return (float)v; }
+__device__ __forceinline__ float tof(DF v) { return v.hi + v.lo; }
+__device__ __forceinline__ double tod(double v) { return v; }
+
+__device__ __forceinline__ void acc_set(float &a, float v) { a = v; }
+__device__ __forceinline__ void acc_set(double &a, float v) { a = v; }
+__device__ __forceinline__ void acc_set(double &a, double v) { a = v; }
+__device__ __forceinline__ void acc_set(DF &a, float v) { a.hi = v; a.lo = 0.f; }
+
+__device__ __forceinline__ void acc_add(float &a, float d) { a = a + d; }
+__device__ __forceinline__ void acc_add(double &a, float d) { a += (double)d; }
+__device__ __forceinline__ void acc_add(double &a, double d) { a += d; }
+__device__ __forceinline__ void acc_add(DF &a, float d) {
+  const float s = __fadd_rn(a.hi, d);
+  const float bp = __fsub_rn(s, a.hi);
+  const float e = __fadd_rn(__fsub_rn(a.hi, __fsub_rn(s, bp)), __fsub_rn(d, bp));  // exact: a.hi + d - s
+  const float lo = __fadd_rn(a.lo, e);
+  const float hi = __fadd_rn(s, lo);
+  a.lo = __fsub_rn(lo, __fsub_rn(hi, s));
+  a.hi = hi;
+}
+
+// h - a, rounded to float (the Kalman residual against a wide accumulator).
+__device__ __forceinline__ float acc_res(float h, float a) { return h - a; }
+__device__ __forceinline__ float acc_res(float h, double a) { return (float)((double)h - a); }
+__device__ __forceinline__ float acc_res(float h, DF a) { return __fsub_rn(__fsub_rn(h, a.hi), a.lo); }
+__device__ __forceinline__ double acc_res(double h, double a) { return h - a; }
+
+// ---------------------------------------------------------------------------
+// sin / cos / versine
+// ---------------------------------------------------------------------------
+// Taylor series about 0 for |a| <= 0.5: sin(a) = a - a^3/3! + ... + a^9/9!
+// (truncation < a^11/11! ~ 1.2e-11 relative) and the versine
+// 1 - cos(a) = a^2/2! - a^4/4! + ... - a^10/10! (truncation < a^12/12!).
+// The coefficients are (-1)^n/(2n+1)! and (-1)^n/(2n)!, rounded to float.
+__device__ __forceinline__ void sv_series(float a, float *s, float *v) {
+  const float a2 = a * a;
+  float ps = fmaf(a2, 2.7557319e-6f, -1.9841270e-4f);
+  ps = fmaf(a2, ps, 8.3333333e-3f);
+  ps = fmaf(a2, ps, -1.6666667e-1f);
+  *s = fmaf(a * a2, ps, a);
+  float pv = fmaf(a2, 2.7557319e-7f, -2.4801587e-5f);
+  pv = fmaf(a2, pv, 1.3888889e-3f);
+  pv = fmaf(a2, pv, -4.1666667e-2f);
+  pv = fmaf(a2, pv, 0.5f);
+  *v = a2 * pv;
+}
+
+// sin(a) and 1 - cos(a) without cancellation.
+template <int SC>
+__device__ __forceinline__ void sin_versine(float a, float *s, float *v) {
+  if (SC == SC_FAST && fabsf(a) <= 0.5f) {
+    sv_series(a, s, v);
+  } else {
+    float sh, ch;
+    sincosf(0.5f * a, &sh, &ch);
+    *s = 2.f * sh * ch;
+    *v = 2.f * sh * sh;
+  }
+}
+
+// Angles phi and theta: MUFU approximation (absolute error ~2^-21 for
+// |x| <= pi) in the fast policy, CUDA's sincosf otherwise.
+template <int SC>
+__device__ __forceinline__ void sincos_angle(float a, float *s, float *c) {
+  if (SC == SC_FAST) __sincosf(a, s, c);
+  else sincosf(a, s, c);
+}
+
+// sin and cos rounded once from a double evaluation: the correctly rounded
+// float result except within ~1e-16 of a rounding midpoint.
+__device__ __forceinline__ float sinf_cr(float x) { return (float)sin((double)x); }
+__device__ __forceinline__ float cosf_cr(float x) { return (float)cos((double)x); }
+
+// ---------------------------------------------------------------------------
+// Track state in registers
+// ---------------------------------------------------------------------------
+// T: element type of the bulk arithmetic; A: type of the x, y, phi accumulators.
+// Covariance: the 15 live elements, named by (row, column); packed indices in
+// comments.
+template <typename T, typename A>
+struct Trk {
+  A x, y, phi;
+  T z, ipt, theta;
+  T c00, c10, c11;            // 0 1 2
+  T c30, c31, c33;            // 6 7 9
+  T c40, c41, c43, c44;       // 10 11 13 14
+  T c50, c51, c53, c54, c55;  // 15 16 18 19 20
+};
+
+// Helix quantities shared by the parameter update and the Jacobian.  omc and
+// omcC are 1 - cos(alpha) and 1 - cos(cosP*sin(alpha)).
+template <typename T>
+struct Helix {
+  T deltaZ, pt, cosP, sinP, sinT, icosT, icosTk, sina, cosa, omc, sCPs, omcC;
+};
+
+// The Jacobian entries that act on a covariance with zero z row (reference
+// :655-666 without column 2), and those of column 2 for the first layer.
+template <typename T>
+struct Jac {
+  T a3, a4, a5;    // J(0,3) J(0,4) J(0,5)
+  T a9, a10, a11;  // J(1,3) J(1,4) J(1,5)
+  T a27, a29;      // J(4,3) J(4,5)
+};
+
+// ---- FORM_PRECISE -----------------------------------------------------------
+
+// Parameter propagation (reference :627-647).  With SC_FAST, icosT/k is taken
+// as icosT * (1/k): one rounding more than the reference's division.
+template <int SC, typename A>
+__device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
+  Helix<float> h;
+  h.deltaZ = zout - s.z;
+  h.pt = __frcp_rn(s.ipt);
+  float cosT;
+  sincos_angle<SC>(tof(s.phi), &h.sinP, &h.cosP);
+  sincos_angle<SC>(s.theta, &h.sinT, &cosT);
+  const float pxin = h.cosP * h.pt;
+  const float pyin = h.sinP * h.pt;
+  h.icosT = __frcp_rn(cosT);
+  h.icosTk = (SC == SC_FAST) ? h.icosT * ik : __fdiv_rn(h.icosT, k);
+  const float alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
+  sin_versine<SC>(alpha, &h.sina, &h.omc);
+  h.cosa = 1.f - h.omc;
+  acc_add(s.x, k * (pxin * h.sina - pyin * h.omc));
+  acc_add(s.y, k * (pyin * h.sina + pxin * h.omc));
+  s.z = zout;
+  acc_add(s.phi, alpha);
+  sin_versine<SC>(h.cosP * h.sina, &h.sCPs, &h.omcC);
+  return h;
+}
+
+template <typename T>
+__device__ __forceinline__ Jac<T> jacobian_precise(const Helix<T> &h, T k, T ipt) {
+  Jac<T> J;
+  const T one = T(1);
+  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT, cosa = h.cosa, sina = h.sina;
+  const T sC = h.sCPs, omcC = h.omcC;
+  const T icTpt = h.icosT * h.pt, icT2 = h.icosT * h.icosT, pt2 = h.pt * h.pt, kpt = k * h.pt;
+  J.a3 = cosP * sinT * h.deltaZ * cosa * (one - sinP * sC) * icTpt - k * (cosP * sina - sinP * omcC) * pt2;
+  J.a4 = kpt * (-sinP * sina + sinP * sinP * sina * sC - cosP * omcC);
+  J.a5 = cosP * h.deltaZ * cosa * (one - sinP * sC) * icT2;
+  J.a9 = sinT * h.deltaZ * cosa * (cosP * cosP * sC + sinP) * icTpt - k * (sinP * sina + cosP * omcC) * pt2;
+  J.a10 = kpt * (-sinP * omcC - sinP * cosP * sina * sC + cosP * sina);
+  J.a11 = h.deltaZ * cosa * (cosP * cosP * sC + sinP) * icT2;
+  J.a27 = sinT * h.deltaZ * h.icosTk;
+  J.a29 = ipt * h.deltaZ * (h.icosT * h.icosTk);
+  return J;
+}
+
+// ---- FORM_REFERENCE ---------------------------------------------------------
+
+// The reference's propagateToZ scalars with its types: the double literals
+// promote the marked sub-expressions to double; sin/cos correctly rounded
+// (the reference calls the C library's sinf/cosf).
+__device__ __forceinline__ Helix<float> propagate_params_ref(Trk<float, float> &s, float zout, float k) {
+  Helix<float> h;
+  h.deltaZ = zout - s.z;
+  h.pt = 1. / s.ipt;
+  h.cosP = cosf_cr(s.phi);
+  h.sinP = sinf_cr(s.phi);
+  const float cosT = cosf_cr(s.theta);
+  h.sinT = sinf_cr(s.theta);
+  const float pxin = h.cosP * h.pt;
+  const float pyin = h.sinP * h.pt;
+  h.icosT = 1.0 / cosT;
+  h.icosTk = h.icosT / k;
+  const float alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
+  h.sina = sinf_cr(alpha);
+  h.cosa = cosf_cr(alpha);
+  s.x = s.x + k * (pxin * h.sina - pyin * (1. - h.cosa));
+  s.y = s.y + k * (pyin * h.sina + pxin * (1. - h.cosa));
+  s.z = zout;
+  s.phi = s.phi + alpha;
+  h.sCPs = sinf_cr(h.cosP * h.sina);
+  const float cC = cosf_cr(h.cosP * h.sina);
+  h.omcC = cC;  // FORM_REFERENCE keeps cos(cosP*sina) itself here
+  h.omc = 0.f;
+  return h;
+}
+
+__device__ __forceinline__ Jac<float> jacobian_ref(const Helix<float> &h, float k, float ipt) {
+  Jac<float> J;
+  const float cosP = h.cosP, sinP = h.sinP, sinT = h.sinT, cosa = h.cosa, sina = h.sina;
+  const float sCosPsina = h.sCPs, cCosPsina = h.omcC;
+  const float deltaZ = h.deltaZ, icosT = h.icosT, icosTk = h.icosTk, pt = h.pt;
+  J.a3 = cosP * sinT * deltaZ * cosa * (1. - sinP * sCosPsina) * (icosT * pt) -
+         k * (cosP * sina - sinP * (1. - cCosPsina)) * (pt * pt);
+  J.a4 = (k * pt) * (-sinP * sina + sinP * sinP * sina * sCosPsina - cosP * (1. - cCosPsina));
+  J.a5 = cosP * deltaZ * cosa * (1. - sinP * sCosPsina) * (icosT * icosT);
+  J.a9 = sinT * deltaZ * cosa * (cosP * cosP * sCosPsina + sinP) * (icosT * pt) -
+         k * (sinP * sina + cosP * (1. - cCosPsina)) * (pt * pt);
+  J.a10 = (k * pt) * (-sinP * (1. - cCosPsina) - sinP * cosP * sina * sCosPsina + cosP * sina);
+  J.a11 = deltaZ * cosa * (cosP * cosP * sCosPsina + sinP) * (icosT * icosT);
+  J.a27 = sinT * deltaZ * (icosTk);
+  J.a29 = ipt * deltaZ * (icosT * icosTk);
+  return J;
+}
+
+// ---- FP64 everything --------------------------------------------------------
+
+__device__ __forceinline__ Helix<double> propagate_params_f64(Trk<double, double> &s, double zout, double k) {
+  Helix<double> h;
+  h.deltaZ = zout - s.z;
+  h.pt = 1.0 / s.ipt;
+  double cosT;
+  sincos(s.phi, &h.sinP, &h.cosP);
+  sincos(s.theta, &h.sinT, &cosT);
+  const double pxin = h.cosP * h.pt, pyin = h.sinP * h.pt;
+  h.icosT = 1.0 / cosT;
+  h.icosTk = h.icosT / k;
+  const double alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
+  sincos(alpha, &h.sina, &h.cosa);
+  h.omc = 1.0 - h.cosa;
+  s.x += k * (pxin * h.sina - pyin * h.omc);
+  s.y += k * (pyin * h.sina + pxin * h.omc);
+  s.z = zout;
+  s.phi += alpha;
+  double cC;
+  sincos(h.cosP * h.sina, &h.sCPs, &cC);
+  h.omcC = 1.0 - cC;
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// Covariance propagation C' = J C J^T
+// ---------------------------------------------------------------------------
+
+// Reduced form: C with zero z row/column.  Sums in the reference's order
+// (t<n>: element n of T = J C row-major; c<n>: packed output n).
+template <typename T, typename A>
+__device__ __forceinline__ void propagate_cov_reduced(Trk<T, A> &s, const Jac<T> &J) {
+  // T = J C, rows 0, 1 and 4 (rows 3 and 5 are C's, row 2 is zero)
+  const T t0 = s.c00 + J.a3 * s.c30 + J.a4 * s.c40 + J.a5 * s.c50;
+  const T t3 = s.c30 + J.a3 * s.c33 + J.a4 * s.c43 + J.a5 * s.c53;
+  const T t4 = s.c40 + J.a3 * s.c43 + J.a4 * s.c44 + J.a5 * s.c54;
+  const T t5 = s.c50 + J.a3 * s.c53 + J.a4 * s.c54 + J.a5 * s.c55;
+  const T t6 = s.c10 + J.a9 * s.c30 + J.a10 * s.c40 + J.a11 * s.c50;
+  const T t7 = s.c11 + J.a9 * s.c31 + J.a10 * s.c41 + J.a11 * s.c51;
+  const T t9 = s.c31 + J.a9 * s.c33 + J.a10 * s.c43 + J.a11 * s.c53;
+  const T t10 = s.c41 + J.a9 * s.c43 + J.a10 * s.c44 + J.a11 * s.c54;
+  const T t11 = s.c51 + J.a9 * s.c53 + J.a10 * s.c54 + J.a11 * s.c55;
+  const T t24 = J.a27 * s.c30 + s.c40 + J.a29 * s.c50;
+  const T t25 = J.a27 * s.c31 + s.c41 + J.a29 * s.c51;
+  const T t27 = J.a27 * s.c33 + s.c43 + J.a29 * s.c53;
+  const T t28 = J.a27 * s.c43 + s.c44 + J.a29 * s.c54;
+  const T t29 = J.a27 * s.c53 + s.c54 + J.a29 * s.c55;
+  const T t18 = s.c30, t19 = s.c31, t21 = s.c33, t22 = s.c43, t23 = s.c53;
+  const T t30 = s.c50, t31 = s.c51, t33 = s.c53, t34 = s.c54, t35 = s.c55;
+  // C' = T J^T
+  s.c00 = t0 + t3 * J.a3 + t4 * J.a4 + t5 * J.a5;        // c0
+  s.c10 = t6 + t9 * J.a3 + t10 * J.a4 + t11 * J.a5;      // c1
+  s.c11 = t7 + t9 * J.a9 + t10 * J.a10 + t11 * J.a11;    // c2
+  s.c30 = t18 + t21 * J.a3 + t22 * J.a4 + t23 * J.a5;    // c6
+  s.c31 = t19 + t21 * J.a9 + t22 * J.a10 + t23 * J.a11;  // c7
+  s.c33 = t21;                                           // c9
+  s.c40 = t24 + t27 * J.a3 + t28 * J.a4 + t29 * J.a5;    // c10
+  s.c41 = t25 + t27 * J.a9 + t28 * J.a10 + t29 * J.a11;  // c11
+  s.c43 = t27;                                           // c13
+  s.c44 = t27 * J.a27 + t28 + t29 * J.a29;               // c14
+  s.c50 = t30 + t33 * J.a3 + t34 * J.a4 + t35 * J.a5;    // c15
+  s.c51 = t31 + t33 * J.a9 + t34 * J.a10 + t35 * J.a11;  // c16
+  s.c53 = t33;                                           // c18
+  s.c54 = t33 * J.a27 + t34 + t35 * J.a29;               // c19
+  s.c55 = t35;                                           // c20
+}
+
+// General form on the full 21-element input covariance b[] (the first
+// propagation of a track), including the Jacobian's z column a2 = J(0,2),
+// a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663).
+template <typename T, typename A>
+__device__ __forceinline__ void propagate_cov_general(Trk<T, A> &s, const T (&b)[21], const Helix<T> &h,
+                                                      const Jac<T> &J) {
+  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT, cosa = h.cosa;
+  const T a2 = cosP * sinT * (sinP * cosa * h.sCPs - cosa) * h.icosT;
+  const T a8 = cosa * sinT * (cosP * cosP * h.sCPs - sinP) * h.icosT;
+  const T a26 = -s.ipt * sinT * h.icosTk;
+  const T a3 = J.a3, a4 = J.a4, a5 = J.a5, a9 = J.a9, a10 = J.a10, a11 = J.a11, a27 = J.a27, a29 = J.a29;
+  const T t0 = b[0] + a2 * b[3] + a3 * b[6] + a4 * b[10] + a5 * b[15];
+  const T t2 = b[3] + a2 * b[5] + a3 * b[8] + a4 * b[12] + a5 * b[17];
+  const T t3 = b[6] + a2 * b[8] + a3 * b[9] + a4 * b[13] + a5 * b[18];
+  const T t4 = b[10] + a2 * b[12] + a3 * b[13] + a4 * b[14] + a5 * b[19];
+  const T t5 = b[15] + a2 * b[17] + a3 * b[18] + a4 * b[19] + a5 * b[20];
+  const T t6 = b[1] + a8 * b[3] + a9 * b[6] + a10 * b[10] + a11 * b[15];
+  const T t7 = b[2] + a8 * b[4] + a9 * b[7] + a10 * b[11] + a11 * b[16];
+  const T t8 = b[4] + a8 * b[5] + a9 * b[8] + a10 * b[12] + a11 * b[17];
+  const T t9 = b[7] + a8 * b[8] + a9 * b[9] + a10 * b[13] + a11 * b[18];
+  const T t10 = b[11] + a8 * b[12] + a9 * b[13] + a10 * b[14] + a11 * b[19];
+  const T t11 = b[16] + a8 * b[17] + a9 * b[18] + a10 * b[19] + a11 * b[20];
+  const T t18 = b[6], t19 = b[7], t20 = b[8], t21 = b[9], t22 = b[13], t23 = b[18];
+  const T t24 = a26 * b[3] + a27 * b[6] + b[10] + a29 * b[15];
+  const T t25 = a26 * b[4] + a27 * b[7] + b[11] + a29 * b[16];
+  const T t26 = a26 * b[5] + a27 * b[8] + b[12] + a29 * b[17];
+  const T t27 = a26 * b[8] + a27 * b[9] + b[13] + a29 * b[18];
+  const T t28 = a26 * b[12] + a27 * b[13] + b[14] + a29 * b[19];
+  const T t29 = a26 * b[17] + a27 * b[18] + b[19] + a29 * b[20];
+  const T t30 = b[15], t31 = b[16], t32 = b[17], t33 = b[18], t34 = b[19], t35 = b[20];
+  s.c00 = t0 + t2 * a2 + t3 * a3 + t4 * a4 + t5 * a5;
+  s.c10 = t6 + t8 * a2 + t9 * a3 + t10 * a4 + t11 * a5;
+  s.c11 = t7 + t8 * a8 + t9 * a9 + t10 * a10 + t11 * a11;
+  s.c30 = t18 + t20 * a2 + t21 * a3 + t22 * a4 + t23 * a5;
+  s.c31 = t19 + t20 * a8 + t21 * a9 + t22 * a10 + t23 * a11;
+  s.c33 = t21;
+  s.c40 = t24 + t26 * a2 + t27 * a3 + t28 * a4 + t29 * a5;
+  s.c41 = t25 + t26 * a8 + t27 * a9 + t28 * a10 + t29 * a11;
+  s.c43 = t27;
+  s.c44 = t26 * a26 + t27 * a27 + t28 + t29 * a29;
+  s.c50 = t30 + t32 * a2 + t33 * a3 + t34 * a4 + t35 * a5;
+  s.c51 = t31 + t32 * a8 + t33 * a9 + t34 * a10 + t35 * a11;
+  s.c53 = t33;
+  s.c54 = t32 * a26 + t33 * a27 + t34 + t35 * a29;
+  s.c55 = t35;
+}
+
+// ---------------------------------------------------------------------------
+// Measurement updates
+// ---------------------------------------------------------------------------
+
+// Compensated a*d - b*c (Kahan's algorithm with one FMA error term).
+__device__ __forceinline__ float det2_comp(float a, float b, float c, float d) {
+  const float w = b * c;
+  const float e = fmaf(-b, c, w);  // exact: w - b*c
+  const float f = fmaf(a, d, -w);
+  return f + e;
+}
+
+// Apply the 2-D (x,y) gain: K(i,:) = (C(i,0), C(i,1)) * Rinv for the live rows
+// (the z row is zero), the parameter update with the residual (hx - x,
+// hy - y), and C - K (H C) (reference :534-617).
+template <typename T, typename A, int FORM>
+__device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r11, T hx, T hy) {
+  const T K0 = s.c00 * r00 + s.c10 * r01, K1 = s.c00 * r01 + s.c10 * r11;
+  const T K2 = s.c10 * r00 + s.c11 * r01, K3 = s.c10 * r01 + s.c11 * r11;
+  const T K6 = s.c30 * r00 + s.c31 * r01, K7 = s.c30 * r01 + s.c31 * r11;
+  const T K8 = s.c40 * r00 + s.c41 * r01, K9 = s.c40 * r01 + s.c41 * r11;
+  const T K10 = s.c50 * r00 + s.c51 * r01, K11 = s.c50 * r01 + s.c51 * r11;
+  const T res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
+  if (FORM == FORM_REFERENCE) {
+    // reference order: p + K0*r0 + K1*r1, left to right
+    acc_set(s.x, tof(s.x) + K0 * res0 + K1 * res1);
+    acc_set(s.y, tof(s.y) + K2 * res0 + K3 * res1);
+    acc_set(s.phi, tof(s.phi) + K8 * res0 + K9 * res1);
+  } else {
+    acc_add(s.x, K0 * res0 + K1 * res1);
+    acc_add(s.y, K2 * res0 + K3 * res1);
+    acc_add(s.phi, K8 * res0 + K9 * res1);
+  }
+  s.ipt = s.ipt + K6 * res0 + K7 * res1;
+  s.theta = s.theta + K10 * res0 + K11 * res1;
+  const T e0 = K0 * s.c00 + K1 * s.c10;
+  const T e1 = K2 * s.c00 + K3 * s.c10;
+  const T e2 = K2 * s.c10 + K3 * s.c11;
+  const T e6 = K6 * s.c00 + K7 * s.c10;
+  const T e7 = K6 * s.c10 + K7 * s.c11;
+  const T e9 = K6 * s.c30 + K7 * s.c31;
+  const T e10 = K8 * s.c00 + K9 * s.c10;
+  const T e11 = K8 * s.c10 + K9 * s.c11;
+  const T e13 = K8 * s.c30 + K9 * s.c31;
+  const T e14 = K8 * s.c40 + K9 * s.c41;
+  const T e15 = K10 * s.c00 + K11 * s.c10;
+  const T e16 = K10 * s.c10 + K11 * s.c11;
+  const T e18 = K10 * s.c30 + K11 * s.c31;
+  const T e19 = K10 * s.c40 + K11 * s.c41;
+  const T e20 = K10 * s.c50 + K11 * s.c51;
+  s.c00 = s.c00 - e0;  s.c10 = s.c10 - e1;  s.c11 = s.c11 - e2;
+  s.c30 = s.c30 - e6;  s.c31 = s.c31 - e7;  s.c33 = s.c33 - e9;
+  s.c40 = s.c40 - e10; s.c41 = s.c41 - e11; s.c43 = s.c43 - e13; s.c44 = s.c44 - e14;
+  s.c50 = s.c50 - e15; s.c51 = s.c51 - e16; s.c53 = s.c53 - e18; s.c54 = s.c54 - e19; s.c55 = s.c55 - e20;
+}
+
+// KalmanUpdate_v2 (reference :503-620): R = C(xy) + V(xy); det in FP64 from
+// the float entries; 1.f/det as a double division rounded to float.
+// Returns true when det <= 0 (or NaN).
+template <typename A, int FORM>
+__device__ __forceinline__ bool update_v2(Trk<float, A> &s, const float (&hp)[3], const float (&hc)[3]) {
+  float r00 = s.c00 + hc[0];
+  float r01 = s.c10 + hc[1];
+  float r11 = s.c11 + hc[2];
+  const double det = (double)r00 * r11 - (double)r01 * r01;
+  const float sc = 1.f / det;
+  const float tmp = sc * r11;
+  r01 *= -sc;
+  r11 = sc * r00;
+  r00 = tmp;
+  update_v2_apply<float, A, FORM>(s, r00, r01, r11, hp[0], hp[1]);
+  return !(det > 0.0);
+}
+
+// The same 2-D update without FP64: compensated determinant, float reciprocal.
+template <typename A>
+__device__ __forceinline__ bool update_v2_comp(Trk<float, A> &s, const float (&hp)[3], const float (&hc)[3]) {
+  float r00 = s.c00 + hc[0];
+  float r01 = s.c10 + hc[1];
+  float r11 = s.c11 + hc[2];
+  const float det = det2_comp(r00, r01, r01, r11);
+  const float sc = __frcp_rn(det);
+  const float tmp = sc * r11;
+  r01 *= -sc;
+  r11 = sc * r00;
+  r00 = tmp;
+  update_v2_apply<float, A, FORM_PRECISE>(s, r00, r01, r11, hp[0], hp[1]);
+  return !(det > 0.0f);
+}
+
+// FP64 2-D update for the all-FP64 kernel.
+__device__ __forceinline__ bool update_v2_f64(Trk<double, double> &s, const double (&hp)[3], const double (&hc)[3]) {
+  const double r00 = s.c00 + hc[0], r01 = s.c10 + hc[1], r11 = s.c11 + hc[2];
+  const double det = r00 * r11 - r01 * r01;
+  const double id = 1.0 / det;
+  update_v2_apply<double, double, FORM_PRECISE>(s, r11 * id, -r01 * id, r00 * id, hp[0], hp[1]);
+  return !(det > 0.0);
+}
+
+// 3-D (x,y,z) measurement update with a Joseph-form covariance update, in
+// precision U (double: the FP64 island; float: FP64-free with compensated
+// cofactors).  The hit covariance is the packed 3x3 (V00 V10 V11 V20 V21 V22).
+// After a propagation C's z row is zero, so R = [[C00+V00, C10+V10, V20],
+// [., C11+V11, V21], [., ., V22]], the gain's z row is zero and the z
+// residual is exactly 0.
+template <typename U>
+__device__ __forceinline__ U cof2(U a, U b, U c, U d) { return a * d - b * c; }
+template <>
+__device__ __forceinline__ float cof2<float>(float a, float b, float c, float d) { return det2_comp(a, b, c, d); }
+
+template <typename U, typename A>
+__device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float (&hp)[3], const float (&hv)[6]) {
+  const U v00 = hv[0], v10 = hv[1], v11 = hv[2], v20 = hv[3], v21 = hv[4], v22 = hv[5];
+  const U C00 = s.c00, C10 = s.c10, C11 = s.c11, C30 = s.c30, C31 = s.c31, C33 = s.c33;
+  const U C40 = s.c40, C41 = s.c41, C43 = s.c43, C44 = s.c44;
+  const U C50 = s.c50, C51 = s.c51, C53 = s.c53, C54 = s.c54, C55 = s.c55;
+  const U R00 = C00 + v00, R10 = C10 + v10, R11 = C11 + v11, R20 = v20, R21 = v21, R22 = v22;
+  // cofactors of the symmetric R; cof2(a, b, c, d) = a*d - b*c
+  const U A00 = cof2<U>(R11, R21, R21, R22);  // R11*R22 - R21*R21
+  const U A10 = cof2<U>(R20, R10, R22, R21);  // R20*R21 - R10*R22
+  const U A20 = cof2<U>(R10, R20, R11, R21);  // R10*R21 - R20*R11
+  const U A11 = cof2<U>(R00, R20, R20, R22);  // R00*R22 - R20*R20
+  const U A21 = cof2<U>(R20, R00, R21, R10);  // R20*R10 - R00*R21
+  const U A22 = cof2<U>(R00, R10, R10, R11);  // R00*R11 - R10*R10
+  const U det = R00 * A00 + R10 * A10 + R20 * A20;
+  const U id = U(1) / det;
+  const U I00 = A00 * id, I10 = A10 * id, I20 = A20 * id, I11 = A11 * id, I21 = A21 * id, I22 = A22 * id;
+  (void)I22;
+  // K = C H^T R^-1 for the live rows x, y, ipt, phi, theta; (C H^T)(i,:) = (C(i,0), C(i,1), 0).
+  const U K[5][3] = {{C00 * I00 + C10 * I10, C00 * I10 + C10 * I11, C00 * I20 + C10 * I21},
+                     {C10 * I00 + C11 * I10, C10 * I10 + C11 * I11, C10 * I20 + C11 * I21},
+                     {C30 * I00 + C31 * I10, C30 * I10 + C31 * I11, C30 * I20 + C31 * I21},
+                     {C40 * I00 + C41 * I10, C40 * I10 + C41 * I11, C40 * I20 + C41 * I21},
+                     {C50 * I00 + C51 * I10, C50 * I10 + C51 * I11, C50 * I20 + C51 * I21}};
+  // residual: z residual is hz - z = 0 after the propagation to z = hz
+  const float r0 = acc_res(hp[0], s.x), r1 = acc_res(hp[1], s.y);
+  acc_add(s.x, float(K[0][0] * U(r0) + K[0][1] * U(r1)));
+  acc_add(s.y, float(K[1][0] * U(r0) + K[1][1] * U(r1)));
+  s.ipt = float(U(s.ipt) + (K[2][0] * U(r0) + K[2][1] * U(r1)));
+  acc_add(s.phi, float(K[3][0] * U(r0) + K[3][1] * U(r1)));
+  s.theta = float(U(s.theta) + (K[4][0] * U(r0) + K[4][1] * U(r1)));
+  // Joseph form: P = (I - K H) C, C'' = P - P H^T K^T + K V K^T, with
+  // P(i,j) = C(i,j) - K(i,0) C(0,j) - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0.
+  const U Cm[5][5] = {{C00, C10, C30, C40, C50},
+                      {C10, C11, C31, C41, C51},
+                      {C30, C31, C33, C43, C53},
+                      {C40, C41, C43, C44, C54},
+                      {C50, C51, C53, C54, C55}};
+  U P[5][5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) P[i][j] = Cm[i][j] - (K[i][0] * Cm[0][j] + K[i][1] * Cm[1][j]);
+  U KV[5][3];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    KV[i][0] = K[i][0] * v00 + K[i][1] * v10 + K[i][2] * v20;
+    KV[i][1] = K[i][0] * v10 + K[i][1] * v11 + K[i][2] * v21;
+    KV[i][2] = K[i][0] * v20 + K[i][1] * v21 + K[i][2] * v22;
+  }
+  U N[5][5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j)
+      N[i][j] = P[i][j] - (P[i][0] * K[j][0] + P[i][1] * K[j][1]) +
+                (KV[i][0] * K[j][0] + KV[i][1] * K[j][1] + KV[i][2] * K[j][2]);
+  s.c00 = float(N[0][0]); s.c10 = float(N[1][0]); s.c11 = float(N[1][1]);
+  s.c30 = float(N[2][0]); s.c31 = float(N[2][1]); s.c33 = float(N[2][2]);
+  s.c40 = float(N[3][0]); s.c41 = float(N[3][1]); s.c43 = float(N[3][2]); s.c44 = float(N[3][3]);
+  s.c50 = float(N[4][0]); s.c51 = float(N[4][1]); s.c53 = float(N[4][2]); s.c54 = float(N[4][3]);
+  s.c55 = float(N[4][4]);
+  return !(det > U(0));
+}
+
+}  // namespace p2z

@@ -1,0 +1,342 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference itself.  Needs a B200.
+
+Tolerances (stated here, derived from the oracle comparison):
+  * precise form (default) vs the FP64 host oracle: every parameter within
+    1e-5 relative (floors in conftest.PAR_FLOOR), live covariance within 1e-4
+    of sqrt(C_ii C_jj);
+  * reference-rounding form vs the reference built with -ffp-contract=off:
+    bit for bit (both evaluate the same FP32 expressions with the same
+    roundings and correctly rounded sin/cos);
+  * any FP32 result vs the reference's own build (FMA contraction on): within
+    the spread the reference shows between its FMA and no-FMA builds, or
+    within the reference's own distance from FP64, whichever the test states.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, LIVE, cov_rel, par_rel
+
+pytestmark = pytest.mark.gpu
+
+PREC_PAR = 1e-5
+PREC_COV = 1e-4
+
+
+def run(p2z, ctx, trk, hit, nevts, update="v2", flags=0, schedule="auto", mask=None, event_ntrks=None, niter=1,
+        block_threads=0):
+    B = trk.shape[2]
+    nb = trk.shape[0]
+    ntrks = nb * B // nevts if event_ntrks is None else 0
+    cfg = p2z.make_config(bsize=B, nevts=nevts, ntrks=ntrks, nlayer=hit.shape[1], update=update, flags=flags,
+                          schedule=schedule, event_ntrks=event_ntrks, niter=niter, block_threads=block_threads)
+    out = np.empty_like(trk)
+    st = ctx.run(cfg, trk, hit, out, hit_mask=mask)
+    return out, st
+
+
+@pytest.fixture(scope="module")
+def physics(p2z):
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=9600, nlayer=20)
+    return p2z.generate_physics(cfg)
+
+
+# ---------------------------------------------------------------------------
+# precise form vs FP64
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("flags", [0, 0x8], ids=["fast_trig", "accurate_trig"])
+def test_precise_v2_vs_fp64_oracle(p2z, oracle, ctx, physics, flags):
+    trk, hit = physics
+    out, st = run(p2z, ctx, trk, hit, 2, flags=flags)
+    o64 = oracle.run_f64(trk, hit)
+    g = p2z.tracks_to_aos(out)
+    r = par_rel(g["par"], o64[:, :6])
+    c = cov_rel(g["cov"], o64[:, 6:])[:, LIVE]
+    print("precise v2 vs fp64: par max", r.max(0), "cov max", c.max())
+    assert st.singular == 0 and st.updates == trk.shape[0] * 32 * 20
+    assert r.max() <= PREC_PAR
+    assert c.max() <= PREC_COV
+
+
+def test_precise_v2_at_least_as_close_to_fp64_as_reference(p2z, oracle, ctx, physics):
+    """Per track, |gpu - ref| is bounded by the reference's own distance from FP64 plus the precise bound."""
+    if not oracle.ref_available("b32"):
+        pytest.skip("reference build absent")
+    trk, hit = physics
+    out, _ = run(p2z, ctx, trk, hit, 2)
+    ref = p2z.tracks_to_aos(oracle.ref_run(trk, hit, name="b32"))
+    o64 = oracle.run_f64(trk, hit)
+    g = p2z.tracks_to_aos(out)
+    bound = par_rel(ref["par"], o64[:, :6]) * (1 + 1e-6) + 2 * PREC_PAR
+    assert (par_rel(g["par"], ref["par"]) <= bound).all()
+
+
+@pytest.mark.parametrize("update", ["v2_comp", "f64"])
+def test_other_2d_variants_vs_fp64(p2z, oracle, ctx, physics, update):
+    trk, hit = physics
+    out, _ = run(p2z, ctx, trk, hit, 2, update=update)
+    o64 = oracle.run_f64(trk, hit)
+    g = p2z.tracks_to_aos(out)
+    tol_par, tol_cov = (1e-7, 1e-7) if update == "f64" else (PREC_PAR, PREC_COV)
+    assert par_rel(g["par"], o64[:, :6]).max() <= tol_par
+    assert cov_rel(g["cov"], o64[:, 6:])[:, LIVE].max() <= tol_cov
+
+
+@pytest.fixture(scope="module")
+def physics_corr(physics):
+    """Physics hits with x-z and y-z hit correlations (0.3), so the 3-D update
+    differs from the 2-D one."""
+    trk, hit = physics
+    h = hit.copy()
+    v00, v11, v22 = h[:, :, 3, :], h[:, :, 5, :], h[:, :, 8, :]
+    h[:, :, 6, :] = 0.3 * np.sqrt(v00 * v22)
+    h[:, :, 7, :] = -0.3 * np.sqrt(v11 * v22)
+    return trk, h
+
+
+@pytest.mark.parametrize("update", ["3x3_f64", "3x3_comp"])
+def test_3x3_joseph_vs_fp64_oracle(p2z, oracle, ctx, physics_corr, update):
+    trk, hit = physics_corr
+    out, st = run(p2z, ctx, trk, hit, 2, update=update)
+    o64 = oracle.run_f64(trk, hit, update=oracle.UPDATE_3X3_JOSEPH)
+    g = p2z.tracks_to_aos(out)
+    r = par_rel(g["par"], o64[:, :6])
+    c = cov_rel(g["cov"], o64[:, 6:])[:, LIVE]
+    print(update, "par max", r.max(0), "cov max", c.max())
+    assert st.singular == 0
+    assert r.max() <= PREC_PAR
+    assert c.max() <= PREC_COV
+    # and it is a different estimator from the 2-D update on this input
+    o2 = oracle.run_f64(trk, hit)
+    assert par_rel(o2[:, :6], o64[:, :6]).max() > 1e-6
+
+
+# ---------------------------------------------------------------------------
+# reference-rounding form vs the reference itself
+# ---------------------------------------------------------------------------
+
+def _bitdiff(a, b):
+    return int((a.view(np.uint32) != b.view(np.uint32)).sum())
+
+
+def test_reference_rounding_bit_exact_known_answer_input(p2z, oracle, ctx, kat_seed):
+    gold = np.load(GOLDEN / "ref_kat_small.npz")
+    t, h = p2z.prepare(p2z.make_atrk(*kat_seed[0]), p2z.make_ahits(kat_seed[1]), 32, 2, 128, 20)
+    out, _ = run(p2z, ctx, t, h, 2, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    assert _bitdiff(out, gold["out_nofma"]) == 0
+
+
+def test_reference_rounding_bit_exact_physics(p2z, oracle, ctx, physics):
+    trk, hit = physics
+    out, _ = run(p2z, ctx, trk, hit, 2, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    ref = oracle.run_f32(trk, hit)  # == reference built with -ffp-contract=off (test_oracle pins it)
+    nd = _bitdiff(out, ref)
+    print("reference-rounding words differing from the no-FMA reference:", nd, "of", out.size)
+    assert nd == 0
+
+
+def test_reference_rounding_within_reference_fma_spread(p2z, oracle, ctx, physics):
+    if not oracle.ref_available("b32"):
+        pytest.skip("reference build absent")
+    trk, hit = physics
+    out, _ = run(p2z, ctx, trk, hit, 2, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    fma = p2z.tracks_to_aos(oracle.ref_run(trk, hit, name="b32"))
+    nofma = p2z.tracks_to_aos(oracle.ref_run(trk, hit, name="b32_nofma"))
+    spread = par_rel(nofma["par"], fma["par"]).max(0)
+    got = par_rel(p2z.tracks_to_aos(out)["par"], fma["par"]).max(0)
+    print("reference FMA/no-FMA spread", spread, "gpu", got)
+    assert (got <= spread * 1.0001 + 1e-12).all()
+
+
+# ---------------------------------------------------------------------------
+# known-answer block
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("flags", [0, 0x20], ids=["precise", "reference_rounding"])
+def test_known_answer_validation_block(p2z, ctx, kat_seed, flags):
+    """The reference's golden block (logs/propagate_gcc_omp.log:30-40) from the
+    GPU on the full 100 x 9600 known-answer input."""
+    import json
+    gold = json.loads((GOLDEN / "kat_block.json").read_text())["blocks"]["propagate_gcc_omp.log"]
+    t, h = p2z.prepare(p2z.make_atrk(*kat_seed[0]), p2z.make_ahits(kat_seed[1]), 32, 100, 9600, 20)
+    out, _ = run(p2z, ctx, t, h, 100, flags=flags)
+    v = p2z.validate(out, 32, 100, 9600, kat_seed[1][19][0])
+    assert v.nnans == 0 and v.nfail == 0
+    got = {"x": v.avgx, "y": v.avgy, "z": v.avgz, "dx": v.avgdx, "dy": v.avgdy, "pt": v.avgpt, "phi": v.avgphi,
+           "theta": v.avgtheta}
+    print({k: "%f" % x for k, x in got.items()})
+    # printed to 6 decimals; allow the last digit +-2 (FP32 evaluations differ at 1e-7)
+    for k in ("x", "y", "z", "dx", "dy", "phi", "theta"):
+        g = float(gold[k][0] if isinstance(gold[k], list) else gold[k])
+        assert abs(got[k] - g) <= 2.5e-6, (k, got[k], g)
+    assert abs(got["pt"] - float(gold["pt"])) <= (2.5e-6 if flags else 2e-4)
+
+
+# ---------------------------------------------------------------------------
+# layouts, schedules, masks
+# ---------------------------------------------------------------------------
+
+def _relayout(trk, hit, B):
+    """Re-pack AOSOA arrays to batch width B (same track order)."""
+    nb, _, B0 = trk.shape
+    n = nb * B0
+    t = trk.transpose(0, 2, 1).reshape(n, 28)
+    h = hit.transpose(0, 3, 1, 2).reshape(n, hit.shape[1], 9)
+    t2 = np.ascontiguousarray(t.reshape(n // B, B, 28).transpose(0, 2, 1))
+    h2 = np.ascontiguousarray(h.reshape(n // B, B, hit.shape[1], 9).transpose(0, 2, 3, 1))
+    return t2, h2
+
+
+@pytest.mark.parametrize("B", [8, 16, 64])
+def test_bsize_layouts_give_identical_tracks(p2z, ctx, physics, B):
+    trk, hit = physics
+    ref, _ = run(p2z, ctx, trk, hit, 2)
+    t2, h2 = _relayout(trk, hit, B)
+    out, _ = run(p2z, ctx, t2, h2, 2)
+    assert np.array_equal(p2z.tracks_to_aos(out)["par"], p2z.tracks_to_aos(ref)["par"])
+    assert np.array_equal(p2z.tracks_to_aos(out)["cov"], p2z.tracks_to_aos(ref)["cov"])
+
+
+@pytest.mark.parametrize("schedule", ["per_event", "persistent"])
+@pytest.mark.parametrize("block", [64, 256])
+def test_schedules_bitwise_equal(p2z, ctx, physics, schedule, block):
+    trk, hit = physics
+    a, _ = run(p2z, ctx, trk, hit, 2, schedule="flat")
+    b, st = run(p2z, ctx, trk, hit, 2, schedule=schedule, block_threads=block)
+    assert _bitdiff(a, b) == 0
+    if schedule == "per_event":
+        assert st.launches == 2
+
+
+def test_uneven_events_with_masks(p2z, oracle, ctx):
+    counts = np.array([50, 1, 0, 777, 3000, 31, 64], dtype=np.int64)
+    cfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20)
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    p2z.mask_layers(m, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=11)
+    o64 = oracle.run_f64(t, h, mask=m)
+    for sched in ("persistent", "per_event", "flat"):
+        out, st = run(p2z, ctx, t, h, len(counts), mask=m, event_ntrks=counts, schedule=sched)
+        g = p2z.tracks_to_aos(out)
+        real = m != 0
+        assert st.updates == sum(bin(int(x)).count("1") for x in m)
+        assert par_rel(g["par"][real], o64[real, :6]).max() <= PREC_PAR
+        # padding slots pass through untouched
+        assert np.array_equal(out.transpose(0, 2, 1).reshape(-1, 28)[~real].view(np.uint32),
+                              t.transpose(0, 2, 1).reshape(-1, 28)[~real].view(np.uint32))
+    # reference rounding with masks == the oracle's reference-semantics restatement, bit for bit
+    out, _ = run(p2z, ctx, t, h, len(counts), mask=m, event_ntrks=counts, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    assert _bitdiff(out, oracle.run_f32(t, h, mask=m)) == 0
+
+
+def test_uneven_events_without_mask_get_padding_mask(p2z, oracle, ctx):
+    counts = np.array([5, 40, 0, 17], dtype=np.int64)
+    cfg = p2z.make_config(bsize=16, nevts=4, event_ntrks=counts, nlayer=20)
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    a, st = run(p2z, ctx, t, h, 4, event_ntrks=counts)
+    b, _ = run(p2z, ctx, t, h, 4, event_ntrks=counts, mask=m)
+    assert _bitdiff(a, b) == 0
+    assert st.updates == int(counts.sum()) * 20
+
+
+def test_run_device_matches_run(p2z, ctx, physics):
+    import torch
+    trk, hit = physics
+    a, _ = run(p2z, ctx, trk, hit, 2)
+    dt, dh = torch.from_numpy(trk).cuda(), torch.from_numpy(hit).cuda()
+    do = torch.empty_like(dt)
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=9600, nlayer=20, niter=3)
+    st = ctx.run_device(cfg, dt, dh, do)
+    assert st.launches == 3 and st.kernel_ms > 0
+    assert _bitdiff(do.cpu().numpy(), a) == 0
+    # full hit copy gives the same result as the 6-word copy
+    b, _ = run(p2z, ctx, trk, hit, 2, flags=p2z.FLAG_FULL_HITS)
+    assert _bitdiff(a, b) == 0
+
+
+def test_step_device_matches_reference_single_steps(p2z, oracle, ctx, kat_seed):
+    """p2z_step_device (one propagateToZ / KalmanUpdate_v2 on every track) ==
+    the reference's functions, bit for bit against its no-FMA build."""
+    import torch
+    if not oracle.ref_available("b32_nofma"):
+        pytest.skip("reference build absent")
+    t, h = p2z.prepare(p2z.make_atrk(*kat_seed[0]), p2z.make_ahits(kat_seed[1]), 32, 2, 128, 20)
+    ref = oracle.ref_lib("b32_nofma")
+    host = t.copy()
+    dt, dh = torch.from_numpy(t.copy()).cuda(), torch.from_numpy(h).cuda()
+    for layer in range(3):
+        for what in (1, 2):
+            for b in range(host.shape[0]):
+                hb = np.ascontiguousarray(h[b, layer])
+                fn = ref.ref_propagate_batch if what == 1 else ref.ref_update_v2_batch
+                fn(host[b].ctypes.data, hb.ctypes.data)
+            ctx.step_device(32, host.shape[0], dt, dh, 20, layer, what=what)
+            assert _bitdiff(dt.cpu().numpy(), host) == 0, (layer, what)
+
+
+def test_error_paths(p2z, ctx, physics):
+    trk, hit = physics
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=9600, nlayer=20, update="3x3_f64",
+                          flags=p2z.FLAG_REFERENCE_ROUNDING)
+    with pytest.raises(p2z.P2zError) as e:
+        ctx.run(cfg, trk, hit, np.empty_like(trk))
+    assert e.value.status == p2z.UNSUPPORTED
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=9600, nlayer=20)
+    with pytest.raises(p2z.P2zError) as e:
+        ctx.run_device(cfg, 0, 0, 0)
+    assert e.value.status == p2z.BAD_ARG
+    # strict mode reports a singular residual covariance: V = -C(xy) makes R = 0
+    t = trk[:1].copy()
+    h = hit[:1].copy()
+    h[:, :, 3:6, :] = -1e3
+    out = np.empty_like(t)
+    cfg = p2z.make_config(bsize=32, nevts=1, ntrks=32, nlayer=20, flags=p2z.FLAG_STRICT)
+    with pytest.raises(p2z.P2zError) as e:
+        ctx.run(cfg, t, h, out)
+    assert e.value.status == p2z.SINGULAR
+    # without strict mode the run completes (NaNs propagate as in the reference)
+    cfg.flags = 0
+    st = ctx.run(cfg, t, h, out)
+    assert st.singular == 1
+
+
+def test_nonfinite_inputs_propagate_like_reference(p2z, oracle, ctx, physics):
+    trk, hit = physics
+    t = trk[:2].copy()
+    h = hit[:2].copy()
+    t[0, 3, 5] = np.nan       # ipt of one track
+    h[1, 7, 0, 9] = np.inf    # a hit of another
+    out, _ = run(p2z, ctx, t, h, 1, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    ref = oracle.run_f32(t, h)
+    g, r = p2z.tracks_to_aos(out), p2z.tracks_to_aos(ref)
+    assert np.array_equal(~np.isfinite(g["par"]).all(1), ~np.isfinite(r["par"]).all(1))
+    assert (~np.isfinite(g["par"]).all(1)).sum() == 2
+
+
+# ---------------------------------------------------------------------------
+# full size (1000 events x 9600 tracks): size-independent properties
+# ---------------------------------------------------------------------------
+
+def test_full_size_properties(p2z, oracle, ctx):
+    import torch
+    cfg = p2z.make_config(bsize=32, nevts=1000, ntrks=9600, nlayer=20)
+    trk, hit = p2z.generate_physics(cfg)
+    dt, dh = torch.from_numpy(trk).cuda(), torch.from_numpy(hit).cuda()
+    do = torch.empty_like(dt)
+    st = ctx.run_device(cfg, dt, dh, do)
+    assert st.singular == 0 and st.updates == 9600 * 1000 * 20
+    out = do.cpu().numpy()
+    del dt, dh, do
+    g = p2z.tracks_to_aos(out)
+    a = p2z.tracks_to_aos(trk)
+    hh_last = hit[:, 19, 2, :].reshape(-1)
+    assert np.isfinite(g["par"]).all() and np.isfinite(g["cov"]).all()
+    assert np.array_equal(g["q"], a["q"])                 # charge untouched
+    assert np.array_equal(g["par"][:, 2], hh_last)        # z lands on the last hit plane exactly
+    assert (g["cov"][:, [0, 2, 9, 14, 20]] > 0).all()     # variances stay positive
+    assert (g["cov"][:, [3, 4, 5, 8, 12, 17]] == 0).all() # z row/column zero
+    # a sample of whole batches against the FP64 oracle
+    idx = np.random.default_rng(5).choice(trk.shape[0], 128, replace=False)
+    o64 = oracle.run_f64(np.ascontiguousarray(trk[idx]), np.ascontiguousarray(hit[idx]))
+    gs = p2z.tracks_to_aos(np.ascontiguousarray(out[idx]))
+    assert par_rel(gs["par"], o64[:, :6]).max() <= PREC_PAR
