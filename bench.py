@@ -254,7 +254,9 @@ def main():
     torch.cuda.set_device(local)
     p2z = load_p2z()
     ctx = p2z.Context(local)
-    stream = torch.cuda.current_stream()
+    # A stream of our own: its handle is never the legacy default stream (0),
+    # which the C ABI would read as "the context's stream".
+    stream = torch.cuda.Stream()
 
     nev = args.nevts
     cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat")

@@ -269,6 +269,25 @@ typedef struct p2z_validation {
  * (pt~12, phi~1.3, theta~2.8, :784-795) and its divisions by ngood. */
 p2z_status p2z_validate(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
                         p2z_validation *v);
+/* The same block for work split over several processes (one event shard
+ * each): pass 1 (means == NULL) accumulates the sums and counts of the tracks
+ * given; after the caller sums pass-1 partials over all shards (an all-reduce
+ * of the doubles and counts), p2z_validate_means gives the global means; pass 2
+ * (means != NULL) accumulates the squared deviations from them; summing those
+ * and calling p2z_validate_combine yields the block of the whole sample.  This
+ * is the reference's two-pass computation (:758-864) with the passes'
+ * accumulators reduced across shards between them.  No counterpart in the
+ * reference (single process). */
+typedef struct p2z_validation_partial {
+  double sum[9];  /* x, y, z, dx/x, dy/y, dz/z, pt, phi, theta (pass 1) */
+  double sq[6];   /* squared deviations of x, y, z, dx/x, dy/y, dz/z (pass 2) */
+  int64_t nnans, nfail, ngood;
+} p2z_validation_partial;
+p2z_status p2z_validate_partial(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
+                                const double means[6], p2z_validation_partial *acc);
+void p2z_validate_means(const p2z_validation_partial *pass1, double means[6]);
+p2z_status p2z_validate_combine(const p2z_validation_partial *pass1, const p2z_validation_partial *pass2,
+                                p2z_validation *v);
 /* Print it with the reference's exact format (:866-876) to stdout. */
 void p2z_print_validation(const p2z_validation *v);
 /* The machine-readable line of the reference (:756), parsed by its tools

@@ -41,13 +41,14 @@ def host_isa() -> str:
     return "v3"
 
 
-_oracle = None
+_oracle = {}
 
 
-def oracle_lib():
-    global _oracle
-    if _oracle is None:
-        path = ORACLE_DIR / "liboracle.so"
+def oracle_lib(cr_trig: bool = False):
+    """cr_trig: the build whose sinf/cosf are correctly rounded (else the C library's)."""
+    key = bool(cr_trig)
+    if key not in _oracle:
+        path = ORACLE_DIR / ("liboracle_crtrig.so" if key else "liboracle.so")
         if not path.exists():
             raise FileNotFoundError(f"{path} not built (make -C oracle oracle)")
         lib = C.CDLL(str(path))
@@ -60,8 +61,8 @@ def oracle_lib():
         lib.orc_run_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p,
                                     C.c_double, C.c_int]
         lib.orc_run_f64.restype = None
-        _oracle = lib
-    return _oracle
+        _oracle[key] = lib
+    return _oracle[key]
 
 
 def _p(a):
@@ -72,12 +73,12 @@ def kfact_default() -> float:
     return float(oracle_lib().orc_default_kfact())
 
 
-def run_f32(trk: np.ndarray, hits: np.ndarray, mask=None, kfact=None) -> np.ndarray:
+def run_f32(trk: np.ndarray, hits: np.ndarray, mask=None, kfact=None, cr_trig=False) -> np.ndarray:
     """Restatement, reference FP32 semantics.  trk (nb,28,B) float32, hits (nb,nl,9,B)."""
     nb, _, B = trk.shape
     nl = hits.shape[1]
     out = np.empty_like(trk)
-    oracle_lib().orc_run_f32(_p(trk), _p(hits), _p(out), nb, B, nl, _p(mask),
+    oracle_lib(cr_trig).orc_run_f32(_p(trk), _p(hits), _p(out), nb, B, nl, _p(mask),
                              kfact_default() if kfact is None else kfact)
     return out
 
@@ -119,7 +120,9 @@ def ref_available(name: str = "b32") -> bool:
 
 def ref_lib(name: str = "b32"):
     """The reference compiled unchanged; name: b8/b16/b32/b64 (2x128 prepare
-    sizes), kat (100x9600, bsize 32) or b32_nofma (-ffp-contract=off)."""
+    sizes), kat (100x9600, bsize 32), b32_nofma (-ffp-contract=off) or
+    b32_nofma_crtrig (-ffp-contract=off, sinf/cosf bound to correctly rounded
+    versions)."""
     key = (host_isa(), name)
     if key not in _refs:
         path = REF_DIR / key[0] / f"libp2zref_{name}.so"

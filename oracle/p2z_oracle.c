@@ -51,6 +51,16 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Built twice: with the C library's sinf/cosf (the reference's own calls) and,
+ * with -DORC_CR_TRIG, with correctly rounded sin/cos (a double evaluation
+ * rounded once to float). */
+#ifdef ORC_CR_TRIG
+static inline float orc_sinf(float x) { return (float)sin((double)x); }
+static inline float orc_cosf(float x) { return (float)cos((double)x); }
+#define sinf orc_sinf
+#define cosf orc_cosf
+#endif
+
 #define ORC_NPAR 6
 #define ORC_NCOV 21
 #define ORC_TRK_WORDS 28 /* 6 par + 21 cov + 1 charge, per track, per batch lane */

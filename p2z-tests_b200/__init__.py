@@ -19,7 +19,8 @@ import pathlib
 import numpy as np
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent
-LIB_PATH = PKG_DIR / "libp2z.so"
+# P2Z_LIBRARY selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = pathlib.Path(os.environ.get("P2Z_LIBRARY", PKG_DIR / "libp2z.so"))
 INCLUDE_H = PKG_DIR.parent / "include" / "p2z.h"
 
 ABI_VERSION = 1
@@ -45,6 +46,7 @@ FLAG_STRICT = 0x2
 FLAG_NO_GRAPH = 0x4
 FLAG_ACCURATE_TRIG = 0x8
 FLAG_FULL_HITS = 0x10
+FLAG_REFERENCE_ROUNDING = 0x20
 
 
 class P2zError(RuntimeError):
@@ -95,6 +97,23 @@ class Validation(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class ValidationPartial(C.Structure):
+    _fields_ = [("sum", C.c_double * 9), ("sq", C.c_double * 6), ("nnans", C.c_int64), ("nfail", C.c_int64),
+                ("ngood", C.c_int64)]
+
+    def to_array(self) -> np.ndarray:
+        """Doubles and counts as one float64 vector (for an all-reduce)."""
+        return np.array(list(self.sum) + list(self.sq) + [self.nnans, self.nfail, self.ngood], dtype=np.float64)
+
+    @classmethod
+    def from_array(cls, a):
+        p = cls()
+        p.sum[:] = [float(x) for x in a[:9]]
+        p.sq[:] = [float(x) for x in a[9:15]]
+        p.nnans, p.nfail, p.ngood = (int(round(x)) for x in a[15:18])
+        return p
+
+
 # Every symbol include/p2z.h declares, with its ctypes signature.
 _VP, _CVP = C.c_void_p, C.c_void_p
 _SIGS = {
@@ -116,6 +135,11 @@ _SIGS = {
     "p2z_generate_physics": (C.c_int, [C.POINTER(PhysicsParams), C.POINTER(Config), _VP, _VP, _VP]),
     "p2z_mask_layers": (C.c_int, [_VP, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64]),
     "p2z_validate": (C.c_int, [_CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float), C.POINTER(Validation)]),
+    "p2z_validate_partial": (C.c_int, [_CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float),
+                                       C.POINTER(C.c_double), C.POINTER(ValidationPartial)]),
+    "p2z_validate_means": (None, [C.POINTER(ValidationPartial), C.POINTER(C.c_double)]),
+    "p2z_validate_combine": (C.c_int, [C.POINTER(ValidationPartial), C.POINTER(ValidationPartial),
+                                       C.POINTER(Validation)]),
     "p2z_print_validation": (None, [C.POINTER(Validation)]),
     "p2z_print_formatted": (None, [C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int]),
     "p2z_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
@@ -293,6 +317,48 @@ def validate(trk_out: np.ndarray, bsize, nevts, ntrks, hit_last) -> dict:
     hl = (C.c_float * 3)(*[float(x) for x in hit_last])
     _check(lib.p2z_validate(_ptr(trk_out), bsize, nevts, ntrks, hl, C.byref(v)))
     return v
+
+
+def validate_sharded(trk_out: np.ndarray, bsize, nevts, ntrks, hit_last, allreduce=None) -> Validation:
+    """Validation block of several event shards (one per process).  `allreduce`
+    sums a float64 vector over all shards in place (e.g. a torch.distributed
+    all-reduce); None means a single shard."""
+    hl = (C.c_float * 3)(*[float(x) for x in hit_last])
+    p1 = ValidationPartial()
+    _check(lib.p2z_validate_partial(_ptr(trk_out), bsize, nevts, ntrks, hl, None, C.byref(p1)))
+    if allreduce is not None:
+        a = p1.to_array()
+        allreduce(a)
+        p1 = ValidationPartial.from_array(a)
+    means = (C.c_double * 6)()
+    lib.p2z_validate_means(C.byref(p1), means)
+    p2 = ValidationPartial()
+    _check(lib.p2z_validate_partial(_ptr(trk_out), bsize, nevts, ntrks, hl, means, C.byref(p2)))
+    if allreduce is not None:
+        a = p2.to_array()
+        allreduce(a)
+        p2 = ValidationPartial.from_array(a)
+    v = Validation()
+    _check(lib.p2z_validate_combine(C.byref(p1), C.byref(p2), C.byref(v)))
+    return v
+
+
+def shard_events(event_ntrks, world: int) -> list[tuple[int, int]]:
+    """Contiguous event ranges [e0, e1) per rank with near-equal track counts
+    (uniform events split evenly by count)."""
+    counts = np.asarray(event_ntrks, dtype=np.int64)
+    total = int(counts.sum())
+    cum = np.concatenate([[0], np.cumsum(counts)])
+    bounds = [0]
+    for r in range(1, world):
+        target = total * r / world
+        e = int(np.searchsorted(cum, target, side="left"))
+        e = max(bounds[-1], min(len(counts), e))
+        if e > 0 and abs(cum[e - 1] - target) < abs(cum[e] - target) and e - 1 >= bounds[-1]:
+            e -= 1
+        bounds.append(e)
+    bounds.append(len(counts))
+    return [(bounds[r], bounds[r + 1]) for r in range(world)]
 
 
 def print_validation(v: Validation):

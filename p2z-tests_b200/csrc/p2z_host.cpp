@@ -342,99 +342,98 @@ p2z_status p2z_mask_layers(uint32_t *hit_mask, int64_t nslots, int nlayer, int m
   return P2Z_OK;
 }
 
-p2z_status p2z_validate(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
-                        p2z_validation *v) {
-  if (!trk_out || !hit_last || !v) return P2Z_BAD_ARG;
+p2z_status p2z_validate_partial(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
+                                const double means[6], p2z_validation_partial *acc) {
+  if (!trk_out || !hit_last || !acc) return P2Z_BAD_ARG;
   if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
   if (nevts < 0 || ntrks < 0 || ntrks % bsize) return P2Z_BAD_ARG;
+  std::memset(acc, 0, sizeof *acc);
   const float *T = (const float *)trk_out;
   const int64_t nb = ntrks / bsize;
-  auto get = [&](int64_t ie, int64_t it, int p) -> float {
-    const int64_t ib = it / bsize;
-    const int lane = (int)(it % bsize);
-    return T[(ib + nb * ie) * (int64_t)TRK_WORDS * bsize + lane + p * bsize];
-  };
   const double hx_ = hit_last[0], hy_ = hit_last[1], hz_ = hit_last[2];
-  // The reference's two passes (src/propagate-toz-test_OMP.cpp:758-864):
-  // skip non-finite tracks, skip tracks outside its fixed window, then
-  // accumulate means and spreads in double over the rest.
-  auto finite6 = [](double a, double b, double c, double d, double e, double f) {
-    return std::isfinite(a) && std::isfinite(b) && std::isfinite(c) && std::isfinite(d) && std::isfinite(e) &&
-           std::isfinite(f);
-  };
-  auto outside = [&](double x_, double y_, double z_, double pt_, double phi_, double theta_) {
-    return std::fabs((x_ - hx_) / hx_) > 1. || std::fabs((y_ - hy_) / hy_) > 1. || std::fabs((z_ - hz_) / hz_) > 1. ||
-           std::fabs((pt_ - 12.) / 12.) > 1. || std::fabs((phi_ - 1.3) / 1.3) > 1. ||
-           std::fabs((theta_ - 2.8) / 2.8) > 1.;
-  };
-  int64_t nnans = 0, nfail = 0, ngood = 0;
-  double avgx = 0, avgy = 0, avgz = 0, avgpt = 0, avgphi = 0, avgtheta = 0, avgdx = 0, avgdy = 0, avgdz = 0;
+  // The reference's track selection (src/propagate-toz-test_OMP.cpp:758-864):
+  // skip non-finite tracks, skip tracks outside its fixed window (pt ~ 12,
+  // phi ~ 1.3, theta ~ 2.8, positions within 100% of the last seed hit).
   for (int64_t ie = 0; ie < nevts; ++ie)
     for (int64_t it = 0; it < ntrks; ++it) {
-      const double x_ = get(ie, it, 0), y_ = get(ie, it, 1), z_ = get(ie, it, 2);
-      const double pt_ = 1. / get(ie, it, 3), phi_ = get(ie, it, 4), theta_ = get(ie, it, 5);
-      if (!finite6(x_, y_, z_, pt_, phi_, theta_)) {
-        nnans++;
+      const float *b = T + ((it / bsize) + nb * ie) * (int64_t)TRK_WORDS * bsize + (it % bsize);
+      const double x_ = b[0], y_ = b[bsize], z_ = b[2 * bsize];
+      const double pt_ = 1. / b[3 * bsize], phi_ = b[4 * bsize], theta_ = b[5 * bsize];
+      if (!(std::isfinite(x_) && std::isfinite(y_) && std::isfinite(z_) && std::isfinite(pt_) &&
+            std::isfinite(phi_) && std::isfinite(theta_))) {
+        acc->nnans++;
         continue;
       }
-      if (outside(x_, y_, z_, pt_, phi_, theta_)) {
-        nfail++;
+      if (std::fabs((x_ - hx_) / hx_) > 1. || std::fabs((y_ - hy_) / hy_) > 1. || std::fabs((z_ - hz_) / hz_) > 1. ||
+          std::fabs((pt_ - 12.) / 12.) > 1. || std::fabs((phi_ - 1.3) / 1.3) > 1. ||
+          std::fabs((theta_ - 2.8) / 2.8) > 1.) {
+        acc->nfail++;
         continue;
       }
-      avgpt += pt_;
-      avgphi += phi_;
-      avgtheta += theta_;
-      avgx += x_;
-      avgy += y_;
-      avgz += z_;
-      avgdx += (x_ - hx_) / x_;
-      avgdy += (y_ - hy_) / y_;
-      avgdz += (z_ - hz_) / z_;
-      ngood++;
+      const double dx = (x_ - hx_) / x_, dy = (y_ - hy_) / y_, dz = (z_ - hz_) / z_;
+      if (!means) {
+        acc->sum[0] += x_;
+        acc->sum[1] += y_;
+        acc->sum[2] += z_;
+        acc->sum[3] += dx;
+        acc->sum[4] += dy;
+        acc->sum[5] += dz;
+        acc->sum[6] += pt_;
+        acc->sum[7] += phi_;
+        acc->sum[8] += theta_;
+      } else {
+        acc->sq[0] += (x_ - means[0]) * (x_ - means[0]);
+        acc->sq[1] += (y_ - means[1]) * (y_ - means[1]);
+        acc->sq[2] += (z_ - means[2]) * (z_ - means[2]);
+        acc->sq[3] += (dx - means[3]) * (dx - means[3]);
+        acc->sq[4] += (dy - means[4]) * (dy - means[4]);
+        acc->sq[5] += (dz - means[5]) * (dz - means[5]);
+      }
+      acc->ngood++;
     }
-  avgpt /= double(ngood);
-  avgphi /= double(ngood);
-  avgtheta /= double(ngood);
-  avgx /= double(ngood);
-  avgy /= double(ngood);
-  avgz /= double(ngood);
-  avgdx /= double(ngood);
-  avgdy /= double(ngood);
-  avgdz /= double(ngood);
-  double stdx = 0, stdy = 0, stdz = 0, stddx = 0, stddy = 0, stddz = 0;
-  for (int64_t ie = 0; ie < nevts; ++ie)
-    for (int64_t it = 0; it < ntrks; ++it) {
-      const double x_ = get(ie, it, 0), y_ = get(ie, it, 1), z_ = get(ie, it, 2);
-      const double pt_ = 1. / get(ie, it, 3), phi_ = get(ie, it, 4), theta_ = get(ie, it, 5);
-      if (!finite6(x_, y_, z_, pt_, phi_, theta_)) continue;
-      if (outside(x_, y_, z_, pt_, phi_, theta_)) continue;
-      stdx += (x_ - avgx) * (x_ - avgx);
-      stdy += (y_ - avgy) * (y_ - avgy);
-      stdz += (z_ - avgz) * (z_ - avgz);
-      stddx += ((x_ - hx_) / x_ - avgdx) * ((x_ - hx_) / x_ - avgdx);
-      stddy += ((y_ - hy_) / y_ - avgdy) * ((y_ - hy_) / y_ - avgdy);
-      stddz += ((z_ - hz_) / z_ - avgdz) * ((z_ - hz_) / z_ - avgdz);
-    }
-  // The reference takes these roots with sqrtf, i.e. in single precision.
-  v->stdx = sqrtf((float)(stdx / double(ngood)));
-  v->stdy = sqrtf((float)(stdy / double(ngood)));
-  v->stdz = sqrtf((float)(stdz / double(ngood)));
-  v->stddx = sqrtf((float)(stddx / double(ngood)));
-  v->stddy = sqrtf((float)(stddy / double(ngood)));
-  v->stddz = sqrtf((float)(stddz / double(ngood)));
-  v->avgx = avgx;
-  v->avgy = avgy;
-  v->avgz = avgz;
-  v->avgdx = avgdx;
-  v->avgdy = avgdy;
-  v->avgdz = avgdz;
-  v->avgpt = avgpt;
-  v->avgphi = avgphi;
-  v->avgtheta = avgtheta;
-  v->nnans = nnans;
-  v->nfail = nfail;
-  v->ngood = ngood;
   return P2Z_OK;
+}
+
+void p2z_validate_means(const p2z_validation_partial *p1, double means[6]) {
+  for (int i = 0; i < 6; ++i) means[i] = p1->sum[i] / double(p1->ngood);
+}
+
+p2z_status p2z_validate_combine(const p2z_validation_partial *p1, const p2z_validation_partial *p2, p2z_validation *v) {
+  if (!p1 || !p2 || !v) return P2Z_BAD_ARG;
+  const double n = double(p1->ngood);
+  v->avgx = p1->sum[0] / n;
+  v->avgy = p1->sum[1] / n;
+  v->avgz = p1->sum[2] / n;
+  v->avgdx = p1->sum[3] / n;
+  v->avgdy = p1->sum[4] / n;
+  v->avgdz = p1->sum[5] / n;
+  v->avgpt = p1->sum[6] / n;
+  v->avgphi = p1->sum[7] / n;
+  v->avgtheta = p1->sum[8] / n;
+  // The reference takes these roots with sqrtf, i.e. in single precision.
+  v->stdx = sqrtf((float)(p2->sq[0] / n));
+  v->stdy = sqrtf((float)(p2->sq[1] / n));
+  v->stdz = sqrtf((float)(p2->sq[2] / n));
+  v->stddx = sqrtf((float)(p2->sq[3] / n));
+  v->stddy = sqrtf((float)(p2->sq[4] / n));
+  v->stddz = sqrtf((float)(p2->sq[5] / n));
+  v->nnans = p1->nnans;
+  v->nfail = p1->nfail;
+  v->ngood = p1->ngood;
+  return P2Z_OK;
+}
+
+p2z_status p2z_validate(const void *trk_out, int bsize, int64_t nevts, int64_t ntrks, const float hit_last[3],
+                        p2z_validation *v) {
+  if (!v) return P2Z_BAD_ARG;
+  p2z_validation_partial p1, p2;
+  p2z_status r = p2z_validate_partial(trk_out, bsize, nevts, ntrks, hit_last, nullptr, &p1);
+  if (r != P2Z_OK) return r;
+  double means[6];
+  p2z_validate_means(&p1, means);
+  r = p2z_validate_partial(trk_out, bsize, nevts, ntrks, hit_last, means, &p2);
+  if (r != P2Z_OK) return r;
+  return p2z_validate_combine(&p1, &p2, v);
 }
 
 void p2z_print_validation(const p2z_validation *v) {

@@ -200,9 +200,15 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   if (singular) atomicOr(a.status, 1u);
 }
 
+// Register budget: at most 256 threads per CTA and at least P2Z_MIN_CTAS
+// 256-thread CTAs resident per SM (1 leaves the register count to ptxas).
+#ifndef P2Z_MIN_CTAS
+#define P2Z_MIN_CTAS 1
+#endif
+
 // One launch over slots [slot_begin, slot_end), one thread per slot.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(256) k_flat(RunArgs a) {
+__global__ void __launch_bounds__(256, P2Z_MIN_CTAS) k_flat(RunArgs a) {
   const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= a.slot_end) return;
   process_slot<B, UPD, SC, MASKED>(a, slot);
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(256) k_flat(RunArgs a) {
 // the range is exhausted.  Work items are taken in slot order, so concurrently
 // running warps read neighbouring batches.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(256) k_persistent(RunArgs a) {
+__global__ void __launch_bounds__(256, P2Z_MIN_CTAS) k_persistent(RunArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t nslots = a.slot_end - a.slot_begin;
   const unsigned long long nitems = (unsigned long long)((nslots + 31) / 32);

@@ -118,8 +118,8 @@ __device__ __forceinline__ void sin_versine(float a, float *s, float *v) {
   }
 }
 
-// Angles phi and theta: MUFU approximation (absolute error ~2^-21 for
-// |x| <= pi) in the fast policy, CUDA's sincosf otherwise.
+// Angle phi: MUFU approximation (absolute error ~2^-21 for |x| <= pi) in the
+// fast policy, CUDA's sincosf otherwise.
 template <int SC>
 __device__ __forceinline__ void sincos_angle(float a, float *s, float *c) {
   if (SC == SC_FAST) __sincosf(a, s, c);
@@ -174,7 +174,10 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   h.pt = __frcp_rn(s.ipt);
   float cosT;
   sincos_angle<SC>(tof(s.phi), &h.sinP, &h.cosP);
-  sincos_angle<SC>(s.theta, &h.sinT, &cosT);
+  // theta always through sincosf: alpha is proportional to tan(theta), and the
+  // MUFU approximation's absolute error (~3.6e-7, i.e. ~2e-6 relative at the
+  // small endcap angles) would bias every step of a high-pT track the same way.
+  sincosf(s.theta, &h.sinT, &cosT);
   const float pxin = h.cosP * h.pt;
   const float pyin = h.sinP * h.pt;
   h.icosT = __frcp_rn(cosT);

@@ -117,6 +117,19 @@ def main():
     np.savez_compressed(HERE / "ref_readme_small.npz", out_fma=O.ref_run(t, h, name="b32"),
                         out_nofma=O.ref_run(t, h, name="b32_nofma"),
                         note="reference hot loop on the pseudocode seed, 2 x 128 tracks, smear 1e-5, cov x1")
+    # 6. the validation block of the FP64 host oracle on the full known-answer
+    #    input (100 x 9600): what an exact evaluation of the reference's
+    #    algorithm prints; the golden log's FP32 evaluation differs from it in
+    #    the 5th-6th significant digit.
+    t, h = p2z.prepare(p2z.make_atrk(*trk_seed), p2z.make_ahits(hit_seeds), 32, 100, 9600, 20)
+    o64 = O.run_f64(t, h)
+    a = t.copy()
+    a[:, :27, :] = o64.reshape(t.shape[0], 32, 27).transpose(0, 2, 1).astype(np.float32)
+    v = p2z.validate(a, 32, 100, 9600, hit_seeds[19][0])
+    meta["fp64_block"] = {k: "%f" % getattr(v, k) for k in ("avgx", "avgy", "avgz", "avgdx", "avgdy", "avgpt",
+                                                            "avgphi", "avgtheta")}
+    meta["fp64_block"]["source"] = "FP64 host oracle (oracle/p2z_oracle.c) on the 100 x 9600 known-answer input"
+    (HERE / "kat_block.json").write_text(json.dumps(meta, indent=1) + "\n")
     print("golden fixtures written to", HERE)
 
 
