@@ -295,6 +295,66 @@ void p2z_print_validation(const p2z_validation *v);
 void p2z_print_formatted(int niter, int64_t nevts, int64_t ntrks, int bsize, double wall_s, double setup_s,
                          int nthreads);
 
+/* ---- serving: continuous batching (no counterpart in the reference) -------- */
+
+/* A server owns a device "slot ring" sized by a memory budget: parallel ring
+ * buffers of track batches, output batches, hit batches and masks indexed by
+ * one batch number, so every admitted event occupies one contiguous range of
+ * batches.  A scheduler thread admits submitted events in arrival order while
+ * ring space allows (copying their inputs host->device on a copy stream),
+ * launches every admitted-but-not-yet-launched event together as one group
+ * (the persistent work-queue kernel over the group's contiguous slot range),
+ * copies each event's tracks back on its own completion event and frees ring
+ * space in completion order.  Events that arrive while a group is on the GPU
+ * are copied in meanwhile and form the next group as soon as the number of
+ * groups in flight drops below max_inflight: copies, kernels and read-backs of
+ * different events overlap.  Per-track arithmetic does not depend on the
+ * group, so an event's result is the same alone and in any mix. */
+typedef struct p2z_server p2z_server;
+
+typedef struct p2z_server_config {
+  int32_t abi_version;         /* P2Z_ABI_VERSION */
+  int32_t bsize;               /* AOSOA width of the submitted events */
+  int32_t nlayer;
+  int32_t update;              /* p2z_update_kind */
+  uint32_t flags;              /* P2Z_FLAG_ACCURATE_TRIG / REFERENCE_ROUNDING / FULL_HITS */
+  float kfact;                 /* 0 -> P2Z_KFACT_DEFAULT */
+  int64_t device_budget_bytes; /* size of the slot ring */
+  int32_t max_inflight;        /* launch groups on the GPU at once; 0 -> 2 */
+  int32_t block_threads;       /* 0 -> 128 */
+} p2z_server_config;
+
+typedef struct p2z_request_info {
+  double submit_s, admit_s, launch_s, done_s; /* host steady-clock seconds */
+  int64_t ntrks;
+  int64_t updates;       /* present hits */
+  int32_t group_events;  /* events launched together with this one */
+  int32_t status;        /* p2z_status of the request */
+} p2z_request_info;
+
+p2z_status p2z_server_create(int device, const p2z_server_config *cfg, p2z_server **out);
+/* Waits for every submitted event, then releases the server. */
+p2z_status p2z_server_destroy(p2z_server *srv);
+/* One event of ntrks tracks: trk_in holds ceil(ntrks/bsize) MPTRK batches,
+ * hits nlayer MPHIT per batch, hit_mask (optional) one word per slot; the
+ * updated tracks go to trk_out.  Host buffers (page-locked for asynchronous
+ * copies) must stay valid until the request completes.  Returns at once;
+ * P2Z_OOM if the event alone exceeds the ring. */
+p2z_status p2z_server_submit(p2z_server *srv, const void *trk_in, const void *hits, const uint32_t *hit_mask,
+                             int64_t ntrks, void *trk_out, int64_t *id);
+/* P2Z_OK and the request's timings once it has completed, else P2Z_NOT_READY.
+ * A completed request is released once poll or wait has reported it. */
+p2z_status p2z_server_poll(p2z_server *srv, int64_t id, p2z_request_info *info);
+/* Blocks until the request completes or timeout_s passes (P2Z_TIMEOUT). */
+p2z_status p2z_server_wait(p2z_server *srv, int64_t id, double timeout_s, p2z_request_info *info);
+/* Seconds on the server's clock (the one the request timings use). */
+double p2z_server_now(const p2z_server *srv);
+/* Load replay for measurements: submits nreq events at the given arrival
+ * times (seconds from the call), waits for all of them and fills infos. */
+p2z_status p2z_server_replay(p2z_server *srv, int64_t nreq, const void *const *trk_in, const void *const *hits,
+                             const uint32_t *const *hit_mask, const int64_t *ntrks, void *const *trk_out,
+                             const double *arrival_s, p2z_request_info *infos);
+
 /* ---- host memory helpers ---------------------------------------------------- */
 
 /* Page-locked host allocation (cudaHostAlloc) for fast asynchronous copies. */

@@ -114,6 +114,21 @@ class ValidationPartial(C.Structure):
         return p
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("bsize", C.c_int32), ("nlayer", C.c_int32), ("update", C.c_int32),
+                ("flags", C.c_uint32), ("kfact", C.c_float), ("device_budget_bytes", C.c_int64),
+                ("max_inflight", C.c_int32), ("block_threads", C.c_int32)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("submit_s", C.c_double), ("admit_s", C.c_double), ("launch_s", C.c_double),
+                ("done_s", C.c_double), ("ntrks", C.c_int64), ("updates", C.c_int64), ("group_events", C.c_int32),
+                ("status", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 # Every symbol include/p2z.h declares, with its ctypes signature.
 _VP, _CVP = C.c_void_p, C.c_void_p
 _SIGS = {
@@ -142,6 +157,15 @@ _SIGS = {
                                        C.POINTER(Validation)]),
     "p2z_print_validation": (None, [C.POINTER(Validation)]),
     "p2z_print_formatted": (None, [C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int]),
+    "p2z_server_create": (C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "p2z_server_destroy": (C.c_int, [_VP]),
+    "p2z_server_submit": (C.c_int, [_VP, _CVP, _CVP, _CVP, C.c_int64, _VP, C.POINTER(C.c_int64)]),
+    "p2z_server_poll": (C.c_int, [_VP, C.c_int64, C.POINTER(RequestInfo)]),
+    "p2z_server_wait": (C.c_int, [_VP, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+    "p2z_server_now": (C.c_double, [_VP]),
+    "p2z_server_replay": (C.c_int, [_VP, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_double), C.POINTER(RequestInfo)]),
     "p2z_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
     "p2z_host_free": (C.c_int, [_VP]),
 }
@@ -411,6 +435,79 @@ class Context:
     def step_device(self, bsize, nbatches, d_trk, d_hits, nlayer, layer, what=3, update=UPDATE_V2, kfact=0.0):
         _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
                                    kfact), self.h)
+
+
+class Server:
+    """Continuous-batching server (p2z_server_*).  Host arrays handed to
+    submit() are kept referenced until their request is reported."""
+
+    def __init__(self, device=0, bsize=32, nlayer=20, update=UPDATE_V2, flags=0, budget_bytes=1 << 30,
+                 max_inflight=2, block_threads=0, kfact=0.0):
+        cfg = ServerConfig()
+        cfg.abi_version = ABI_VERSION
+        cfg.bsize = bsize
+        cfg.nlayer = nlayer
+        cfg.update = UPDATE_NAMES.get(update, update) if isinstance(update, str) else update
+        cfg.flags = flags
+        cfg.kfact = kfact
+        cfg.device_budget_bytes = int(budget_bytes)
+        cfg.max_inflight = max_inflight
+        cfg.block_threads = block_threads
+        h = C.c_void_p()
+        _check(lib.p2z_server_create(device, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.bsize = bsize
+        self._keep = {}
+
+    def submit(self, trk, hits, mask, ntrks, out) -> int:
+        rid = C.c_int64()
+        _check(lib.p2z_server_submit(self.h, _ptr(trk), _ptr(hits), _ptr(mask), int(ntrks), _ptr(out), C.byref(rid)))
+        self._keep[rid.value] = (trk, hits, mask, out)
+        return rid.value
+
+    def poll(self, rid):
+        info = RequestInfo()
+        st = lib.p2z_server_poll(self.h, rid, C.byref(info))
+        if st == NOT_READY:
+            return None
+        _check(st)
+        self._keep.pop(rid, None)
+        return info
+
+    def wait(self, rid, timeout=600.0) -> RequestInfo:
+        info = RequestInfo()
+        _check(lib.p2z_server_wait(self.h, rid, timeout, C.byref(info)))
+        self._keep.pop(rid, None)
+        return info
+
+    def now(self) -> float:
+        return lib.p2z_server_now(self.h)
+
+    def replay(self, events, arrivals):
+        """events: list of (trk, hits, mask, ntrks, out); arrivals: seconds from now."""
+        n = len(events)
+        P = C.c_void_p * n
+        trk = P(*[_ptr(e[0]) for e in events])
+        hit = P(*[_ptr(e[1]) for e in events])
+        msk = P(*[_ptr(e[2]) for e in events])
+        ntr = (C.c_int64 * n)(*[int(e[3]) for e in events])
+        out = P(*[_ptr(e[4]) for e in events])
+        arr = (C.c_double * n)(*[float(a) for a in arrivals])
+        infos = (RequestInfo * n)()
+        _check(lib.p2z_server_replay(self.h, n, trk, hit, msk, ntr, out, arr, infos))
+        return list(infos)
+
+    def close(self):
+        if self.h:
+            lib.p2z_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class PinnedArray:

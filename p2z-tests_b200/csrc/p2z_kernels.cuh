@@ -41,11 +41,12 @@ enum { UPDK_V2 = 0, UPDK_V2_COMP = 1, UPDK_3X3_F64 = 2, UPDK_3X3_COMP = 3, UPDK_
 template <int UPD>
 struct Types {
   using T = typename std::conditional<UPD == UPDK_F64, double, float>::type;
+  // x/y accumulators: anchored FP32 offsets (precise forms), float pairs
+  // (V2_COMP), FP64 (F64), plain float (reference rounding).
   using A = typename std::conditional<
       UPD == UPDK_F64, double,
       typename std::conditional<UPD == UPDK_V2_REF, float,
-                                typename std::conditional<UPD == UPDK_V2_COMP || UPD == UPDK_3X3_COMP, DF,
-                                                          double>::type>::type>::type;
+                                typename std::conditional<UPD == UPDK_V2_COMP, DF, AP>::type>::type>::type;
   static constexpr int NH = (UPD == UPDK_3X3_F64 || UPD == UPDK_3X3_COMP) ? 9 : 6;
 };
 
@@ -123,7 +124,7 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
       return update_v2<typename Types<UPD>::A, (UPD == UPDK_V2_REF) ? FORM_REFERENCE : FORM_PRECISE>(s, hp, hc);
     } else if constexpr (UPD == UPDK_V2_COMP) {
       const float hc[3] = {h.w[3], h.w[4], h.w[5]};
-      return update_v2_comp(s, hp, hc);
+      return update_v2<DF, FORM_PRECISE>(s, hp, hc);
     } else {
       const float hv[6] = {h.w[3], h.w[4], h.w[5], h.w[6], h.w[7], h.w[8]};
       if constexpr (UPD == UPDK_3X3_F64) return update_3x3_joseph<double>(s, hp, hv);
@@ -164,23 +165,45 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   acc_set(s.y, in[1]);
   acc_set(s.phi, in[4]);
   s.z = in[2]; s.ipt = in[3]; s.theta = in[5];
+  if constexpr (UPD != UPDK_F64 && UPD != UPDK_V2_REF) init_direction(s);
   T b21[21];
 #pragma unroll
   for (int e = 0; e < 21; ++e) b21[e] = T(in[6 + e]);
 
   bool singular = false;
-  const int l = __ffs(m) - 1;
-  uint32_t rest = m & (m - 1u);
-  HitRegs<NH> h, hn;
-  load_hit<B, NH>(h, hit_lane<B>(a.hits, slot, a.nlayer, l));
-  if (rest) load_hit<B, NH>(hn, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
-  singular |= step<UPD, SC, true>(s, b21, h, k, ik);
-
-  while (rest) {
-    h = hn;
-    rest &= rest - 1u;
-    if (rest) load_hit<B, NH>(hn, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
-    singular |= step<UPD, SC, false>(s, b21, h, k, ik);
+  HitRegs<NH> h0, h1;
+  if constexpr (!MASKED) {
+    // every layer present: counted loop, hits addressed by a running pointer;
+    // two hit buffers alternate so the next layer is in flight during a step
+    const int64_t stride = (int64_t)HIT_WORDS * B;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
+    const int nl = a.nlayer;
+    load_hit<B, NH>(h0, hp);
+    if (nl > 1) load_hit<B, NH>(h1, hp + stride);
+    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    int l = 1;
+    for (; l + 1 < nl; l += 2) {
+      load_hit<B, NH>(h0, hp + (l + 1) * stride);
+      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      if (l + 2 < nl) load_hit<B, NH>(h1, hp + (l + 2) * stride);
+      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+    }
+    if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+  } else {
+    // present layers in order: lowest set bit first
+    uint32_t rest = m & (m - 1u);
+    load_hit<B, NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(m) - 1));
+    if (rest) load_hit<B, NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    while (rest) {
+      rest &= rest - 1u;  // h1 holds the layer just removed from rest
+      if (rest) load_hit<B, NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      if (!rest) break;
+      rest &= rest - 1u;  // h0 holds the layer just removed
+      if (rest) load_hit<B, NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+    }
   }
 
   const float z0 = 0.0f;

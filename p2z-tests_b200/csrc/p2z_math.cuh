@@ -42,6 +42,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace p2z {
 
 enum { SC_ACCURATE = 0, SC_FAST = 1 };
@@ -56,7 +58,17 @@ struct DF {
   float hi, lo;
 };
 
+// An anchored position: the last hit's coordinate a (a float read from
+// memory, exact) plus a float offset u.  Offsets stay of the order of one
+// step, so they round ~10x finer than the coordinate itself, and the Kalman
+// residual (h - a) - u is formed without cancellation error beyond the
+// rounding of h - a.  All FP32, full rate.
+struct AP {
+  float a, u;
+};
+
 __device__ __forceinline__ float tof(float v) { return v; }
+__device__ __forceinline__ float tof(AP v) { return v.a + v.u; }
 __device__ __forceinline__ float tof(double v) { return (float)v; }
 __device__ __forceinline__ float tof(DF v) { return v.hi + v.lo; }
 __device__ __forceinline__ double tod(double v) { return v; }
@@ -65,6 +77,8 @@ __device__ __forceinline__ void acc_set(float &a, float v) { a = v; }
 __device__ __forceinline__ void acc_set(double &a, float v) { a = v; }
 __device__ __forceinline__ void acc_set(double &a, double v) { a = v; }
 __device__ __forceinline__ void acc_set(DF &a, float v) { a.hi = v; a.lo = 0.f; }
+__device__ __forceinline__ void acc_set(AP &a, float v) { a.a = v; a.u = 0.f; }
+__device__ __forceinline__ void acc_add(AP &a, float d) { a.u += d; }
 
 __device__ __forceinline__ void acc_add(float &a, float d) { a = a + d; }
 __device__ __forceinline__ void acc_add(double &a, float d) { a += (double)d; }
@@ -84,6 +98,29 @@ __device__ __forceinline__ float acc_res(float h, float a) { return h - a; }
 __device__ __forceinline__ float acc_res(float h, double a) { return (float)((double)h - a); }
 __device__ __forceinline__ float acc_res(float h, DF a) { return __fsub_rn(__fsub_rn(h, a.hi), a.lo); }
 __device__ __forceinline__ double acc_res(double h, double a) { return h - a; }
+__device__ __forceinline__ float acc_res(float h, AP a) { return (h - a.a) - a.u; }
+
+// After a Kalman update with residual res = h - x and increment inc, the new
+// position is x + inc.  AP re-anchors at the hit: x + inc = h + (inc - res).
+__device__ __forceinline__ void acc_update(AP &a, float h, float res, float inc) {
+  a.a = h;
+  a.u = inc - res;
+}
+template <typename A, typename T>
+__device__ __forceinline__ void acc_update(A &a, T h, T res, T inc) {
+  (void)h;
+  (void)res;
+  acc_add(a, inc);
+}
+
+// Reciprocal: MUFU approximation refined by one Newton-Raphson step,
+// r' = r + r (1 - x r); within about 1 ulp of 1/x for normal x, no branch.
+__device__ __forceinline__ float rcp_nr(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  const float e = fmaf(-x, r, 1.0f);
+  return fmaf(r, e, r);
+}
 
 // ---------------------------------------------------------------------------
 // sin / cos / versine
@@ -131,16 +168,47 @@ __device__ __forceinline__ void sincos_angle(float a, float *s, float *c) {
 __device__ __forceinline__ float sinf_cr(float x) { return (float)sin((double)x); }
 __device__ __forceinline__ float cosf_cr(float x) { return (float)cos((double)x); }
 
+// Rotate the unit vector (c, s) = (cos t, sin t) to t + d:
+// cos(t+d) = c - (c*v + s*w), sin(t+d) = s - (s*v - c*w) with w = sin d and
+// v = 1 - cos d from their series (sv_series; truncation below 1e-11 for
+// |d| <= 0.5 and below 3e-8 for |d| <= 1).  No branch: Kalman corrections to
+// phi and theta are far below 1 rad for any track the filter can follow, and
+// NaN or Inf propagate.
+__device__ __forceinline__ void rotate(float &c, float &s, float d) {
+  float w, v;
+  sv_series(d, &w, &v);
+  const float cn = c - fmaf(c, v, s * w);
+  const float sn = s - fmaf(s, v, -(c * w));
+  c = cn;
+  s = sn;
+}
+
 // ---------------------------------------------------------------------------
 // Track state in registers
 // ---------------------------------------------------------------------------
 // T: element type of the bulk arithmetic; A: type of the x, y, phi accumulators.
 // Covariance: the 15 live elements, named by (row, column); packed indices in
 // comments.
+// phi is carried in a wide float when the positions are anchored (AP): it has
+// no natural anchor, and it is only an output (its cos/sin are rotated).
+template <typename A>
+struct PhiOf {
+  using type = A;
+};
+template <>
+struct PhiOf<AP> {
+  using type = double;
+};
+
 template <typename T, typename A>
 struct Trk {
-  A x, y, phi;
+  A x, y;
+  typename PhiOf<A>::type phi;
   T z, ipt, theta;
+  // FORM_PRECISE carries cos/sin of phi and theta from layer to layer and
+  // rotates them by each step's angle increment (alpha in the propagation, the
+  // Kalman corrections in the update) instead of evaluating sin/cos anew.
+  T cP, sP, cT, sT;
   T c00, c10, c11;            // 0 1 2
   T c30, c31, c33;            // 6 7 9
   T c40, c41, c43, c44;       // 10 11 13 14
@@ -171,16 +239,13 @@ template <int SC, typename A>
 __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
   Helix<float> h;
   h.deltaZ = zout - s.z;
-  h.pt = __frcp_rn(s.ipt);
-  float cosT;
-  sincos_angle<SC>(tof(s.phi), &h.sinP, &h.cosP);
-  // theta always through sincosf: alpha is proportional to tan(theta), and the
-  // MUFU approximation's absolute error (~3.6e-7, i.e. ~2e-6 relative at the
-  // small endcap angles) would bias every step of a high-pT track the same way.
-  sincosf(s.theta, &h.sinT, &cosT);
+  h.pt = rcp_nr(s.ipt);
+  h.cosP = s.cP;
+  h.sinP = s.sP;
+  h.sinT = s.sT;
   const float pxin = h.cosP * h.pt;
   const float pyin = h.sinP * h.pt;
-  h.icosT = __frcp_rn(cosT);
+  h.icosT = rcp_nr(s.cT);
   h.icosTk = (SC == SC_FAST) ? h.icosT * ik : __fdiv_rn(h.icosT, k);
   const float alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
   sin_versine<SC>(alpha, &h.sina, &h.omc);
@@ -190,22 +255,46 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   s.z = zout;
   acc_add(s.phi, alpha);
   sin_versine<SC>(h.cosP * h.sina, &h.sCPs, &h.omcC);
+  // phi advanced by alpha: rotate (cos phi, sin phi) with sin(alpha) and the versine
+  s.cP = h.cosP - fmaf(h.cosP, h.omc, h.sinP * h.sina);
+  s.sP = h.sinP - fmaf(h.sinP, h.omc, -(h.cosP * h.sina));
   return h;
 }
 
+// First evaluation of the carried direction cosines of a track.
+template <typename A>
+__device__ __forceinline__ void init_direction(Trk<float, A> &s) {
+  sincosf(tof(s.phi), &s.sP, &s.cP);
+  sincosf(s.theta, &s.sT, &s.cT);
+}
+
+// The same entries with the shared factors taken out (exact in real
+// arithmetic; fewer products):
+//   B = 1 - sinP*sC,  D = cosP^2*sC + sinP,  u = cosP*dZ*cosa*B,  v = dZ*cosa*D,
+//   J03 = u*sinT*icosT*pt - k*pt^2*(cosP*sina - sinP*omcC)   J05 = u*icosT^2
+//   J13 = v*sinT*icosT*pt - k*pt^2*(sinP*sina + cosP*omcC)   J15 = v*icosT^2
+//   J04 = -k*pt*(sinP*sina*B + cosP*omcC)                     J14 = k*pt*(cosP*sina*B - sinP*omcC)
 template <typename T>
 __device__ __forceinline__ Jac<T> jacobian_precise(const Helix<T> &h, T k, T ipt) {
   Jac<T> J;
-  const T one = T(1);
-  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT, cosa = h.cosa, sina = h.sina;
-  const T sC = h.sCPs, omcC = h.omcC;
-  const T icTpt = h.icosT * h.pt, icT2 = h.icosT * h.icosT, pt2 = h.pt * h.pt, kpt = k * h.pt;
-  J.a3 = cosP * sinT * h.deltaZ * cosa * (one - sinP * sC) * icTpt - k * (cosP * sina - sinP * omcC) * pt2;
-  J.a4 = kpt * (-sinP * sina + sinP * sinP * sina * sC - cosP * omcC);
-  J.a5 = cosP * h.deltaZ * cosa * (one - sinP * sC) * icT2;
-  J.a9 = sinT * h.deltaZ * cosa * (cosP * cosP * sC + sinP) * icTpt - k * (sinP * sina + cosP * omcC) * pt2;
-  J.a10 = kpt * (-sinP * omcC - sinP * cosP * sina * sC + cosP * sina);
-  J.a11 = h.deltaZ * cosa * (cosP * cosP * sC + sinP) * icT2;
+  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT;
+  const T dzc = h.deltaZ * h.cosa;
+  const T B = T(1) - sinP * h.sCPs;
+  const T D = cosP * cosP * h.sCPs + sinP;
+  const T icT2 = h.icosT * h.icosT;
+  const T stp = sinT * (h.icosT * h.pt);
+  const T kpt = k * h.pt;
+  const T kpt2 = kpt * h.pt;
+  const T m1 = cosP * h.sina, m2 = sinP * h.sina;
+  const T n1 = cosP * h.omcC, n2 = sinP * h.omcC;
+  const T u = cosP * dzc * B;
+  const T v = dzc * D;
+  J.a3 = u * stp - kpt2 * (m1 - n2);
+  J.a5 = u * icT2;
+  J.a9 = v * stp - kpt2 * (m2 + n1);
+  J.a11 = v * icT2;
+  J.a4 = -kpt * (m2 * B + n1);
+  J.a10 = kpt * (m1 * B - n2);
   J.a27 = sinT * h.deltaZ * h.icosTk;
   J.a29 = ipt * h.deltaZ * (h.icosT * h.icosTk);
   return J;
@@ -398,71 +487,100 @@ __device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r1
   const T K8 = s.c40 * r00 + s.c41 * r01, K9 = s.c40 * r01 + s.c41 * r11;
   const T K10 = s.c50 * r00 + s.c51 * r01, K11 = s.c50 * r01 + s.c51 * r11;
   const T res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
-  if (FORM == FORM_REFERENCE) {
+  if constexpr (FORM == FORM_REFERENCE) {
     // reference order: p + K0*r0 + K1*r1, left to right
     acc_set(s.x, tof(s.x) + K0 * res0 + K1 * res1);
     acc_set(s.y, tof(s.y) + K2 * res0 + K3 * res1);
     acc_set(s.phi, tof(s.phi) + K8 * res0 + K9 * res1);
+    s.theta = s.theta + K10 * res0 + K11 * res1;
+  } else if constexpr (std::is_same<T, float>::value) {
+    acc_update(s.x, hx, res0, K0 * res0 + K1 * res1);
+    acc_update(s.y, hy, res1, K2 * res0 + K3 * res1);
+    const float dphi = K8 * res0 + K9 * res1;
+    const float dth = K10 * res0 + K11 * res1;
+    acc_add(s.phi, dphi);
+    s.theta = s.theta + dth;
+    rotate(s.cP, s.sP, dphi);
+    rotate(s.cT, s.sT, dth);
   } else {
     acc_add(s.x, K0 * res0 + K1 * res1);
     acc_add(s.y, K2 * res0 + K3 * res1);
     acc_add(s.phi, K8 * res0 + K9 * res1);
+    s.theta = s.theta + K10 * res0 + K11 * res1;
   }
   s.ipt = s.ipt + K6 * res0 + K7 * res1;
-  s.theta = s.theta + K10 * res0 + K11 * res1;
-  const T e0 = K0 * s.c00 + K1 * s.c10;
-  const T e1 = K2 * s.c00 + K3 * s.c10;
-  const T e2 = K2 * s.c10 + K3 * s.c11;
-  const T e6 = K6 * s.c00 + K7 * s.c10;
-  const T e7 = K6 * s.c10 + K7 * s.c11;
-  const T e9 = K6 * s.c30 + K7 * s.c31;
-  const T e10 = K8 * s.c00 + K9 * s.c10;
-  const T e11 = K8 * s.c10 + K9 * s.c11;
-  const T e13 = K8 * s.c30 + K9 * s.c31;
-  const T e14 = K8 * s.c40 + K9 * s.c41;
-  const T e15 = K10 * s.c00 + K11 * s.c10;
-  const T e16 = K10 * s.c10 + K11 * s.c11;
-  const T e18 = K10 * s.c30 + K11 * s.c31;
-  const T e19 = K10 * s.c40 + K11 * s.c41;
-  const T e20 = K10 * s.c50 + K11 * s.c51;
-  s.c00 = s.c00 - e0;  s.c10 = s.c10 - e1;  s.c11 = s.c11 - e2;
-  s.c30 = s.c30 - e6;  s.c31 = s.c31 - e7;  s.c33 = s.c33 - e9;
-  s.c40 = s.c40 - e10; s.c41 = s.c41 - e11; s.c43 = s.c43 - e13; s.c44 = s.c44 - e14;
-  s.c50 = s.c50 - e15; s.c51 = s.c51 - e16; s.c53 = s.c53 - e18; s.c54 = s.c54 - e19; s.c55 = s.c55 - e20;
+  if constexpr (FORM == FORM_PRECISE && std::is_same<T, float>::value) {
+    // C - K (H C), each element as two fused multiply-adds: C - K_i0 C_0j - K_i1 C_1j
+    const T c00 = s.c00, c10 = s.c10, c11 = s.c11, c30 = s.c30, c31 = s.c31, c40 = s.c40, c41 = s.c41;
+    const T c50 = s.c50, c51 = s.c51;
+    s.c00 = fmaf(-K1, c10, fmaf(-K0, c00, c00));
+    s.c10 = fmaf(-K3, c10, fmaf(-K2, c00, c10));
+    s.c11 = fmaf(-K3, c11, fmaf(-K2, c10, c11));
+    s.c30 = fmaf(-K7, c10, fmaf(-K6, c00, c30));
+    s.c31 = fmaf(-K7, c11, fmaf(-K6, c10, c31));
+    s.c33 = fmaf(-K7, c31, fmaf(-K6, c30, s.c33));
+    s.c40 = fmaf(-K9, c10, fmaf(-K8, c00, c40));
+    s.c41 = fmaf(-K9, c11, fmaf(-K8, c10, c41));
+    s.c43 = fmaf(-K9, c31, fmaf(-K8, c30, s.c43));
+    s.c44 = fmaf(-K9, c41, fmaf(-K8, c40, s.c44));
+    s.c50 = fmaf(-K11, c10, fmaf(-K10, c00, c50));
+    s.c51 = fmaf(-K11, c11, fmaf(-K10, c10, c51));
+    s.c53 = fmaf(-K11, c31, fmaf(-K10, c30, s.c53));
+    s.c54 = fmaf(-K11, c41, fmaf(-K10, c40, s.c54));
+    s.c55 = fmaf(-K11, c51, fmaf(-K10, c50, s.c55));
+  } else {
+    const T e0 = K0 * s.c00 + K1 * s.c10;
+    const T e1 = K2 * s.c00 + K3 * s.c10;
+    const T e2 = K2 * s.c10 + K3 * s.c11;
+    const T e6 = K6 * s.c00 + K7 * s.c10;
+    const T e7 = K6 * s.c10 + K7 * s.c11;
+    const T e9 = K6 * s.c30 + K7 * s.c31;
+    const T e10 = K8 * s.c00 + K9 * s.c10;
+    const T e11 = K8 * s.c10 + K9 * s.c11;
+    const T e13 = K8 * s.c30 + K9 * s.c31;
+    const T e14 = K8 * s.c40 + K9 * s.c41;
+    const T e15 = K10 * s.c00 + K11 * s.c10;
+    const T e16 = K10 * s.c10 + K11 * s.c11;
+    const T e18 = K10 * s.c30 + K11 * s.c31;
+    const T e19 = K10 * s.c40 + K11 * s.c41;
+    const T e20 = K10 * s.c50 + K11 * s.c51;
+    s.c00 = s.c00 - e0;  s.c10 = s.c10 - e1;  s.c11 = s.c11 - e2;
+    s.c30 = s.c30 - e6;  s.c31 = s.c31 - e7;  s.c33 = s.c33 - e9;
+    s.c40 = s.c40 - e10; s.c41 = s.c41 - e11; s.c43 = s.c43 - e13; s.c44 = s.c44 - e14;
+    s.c50 = s.c50 - e15; s.c51 = s.c51 - e16; s.c53 = s.c53 - e18; s.c54 = s.c54 - e19; s.c55 = s.c55 - e20;
+  }
 }
 
-// KalmanUpdate_v2 (reference :503-620): R = C(xy) + V(xy); det in FP64 from
-// the float entries; 1.f/det as a double division rounded to float.
+// KalmanUpdate_v2 (reference :503-620): R = C(xy) + V(xy), its inverse by
+// Cramer's rule, gain, parameter and covariance update.
+// FORM_REFERENCE: the determinant in FP64 from the float entries and 1.f/det as
+// a double division rounded to float, as the reference.
+// FORM_PRECISE: Kahan's compensated FP32 determinant (error <= 2 ulp of the
+// exact determinant of the float entries, the same bound as the FP64 product
+// rounded to float) and a correctly rounded float reciprocal -- no FP64.
 // Returns true when det <= 0 (or NaN).
 template <typename A, int FORM>
 __device__ __forceinline__ bool update_v2(Trk<float, A> &s, const float (&hp)[3], const float (&hc)[3]) {
   float r00 = s.c00 + hc[0];
   float r01 = s.c10 + hc[1];
   float r11 = s.c11 + hc[2];
-  const double det = (double)r00 * r11 - (double)r01 * r01;
-  const float sc = 1.f / det;
+  float sc;
+  bool bad;
+  if constexpr (FORM == FORM_REFERENCE) {
+    const double det = (double)r00 * r11 - (double)r01 * r01;
+    sc = 1.f / det;
+    bad = !(det > 0.0);
+  } else {
+    const float det = det2_comp(r00, r01, r01, r11);
+    sc = rcp_nr(det);
+    bad = !(det > 0.0f);
+  }
   const float tmp = sc * r11;
   r01 *= -sc;
   r11 = sc * r00;
   r00 = tmp;
   update_v2_apply<float, A, FORM>(s, r00, r01, r11, hp[0], hp[1]);
-  return !(det > 0.0);
-}
-
-// The same 2-D update without FP64: compensated determinant, float reciprocal.
-template <typename A>
-__device__ __forceinline__ bool update_v2_comp(Trk<float, A> &s, const float (&hp)[3], const float (&hc)[3]) {
-  float r00 = s.c00 + hc[0];
-  float r01 = s.c10 + hc[1];
-  float r11 = s.c11 + hc[2];
-  const float det = det2_comp(r00, r01, r01, r11);
-  const float sc = __frcp_rn(det);
-  const float tmp = sc * r11;
-  r01 *= -sc;
-  r11 = sc * r00;
-  r00 = tmp;
-  update_v2_apply<float, A, FORM_PRECISE>(s, r00, r01, r11, hp[0], hp[1]);
-  return !(det > 0.0f);
+  return bad;
 }
 
 // FP64 2-D update for the all-FP64 kernel.
@@ -511,11 +629,16 @@ __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float 
                      {C50 * I00 + C51 * I10, C50 * I10 + C51 * I11, C50 * I20 + C51 * I21}};
   // residual: z residual is hz - z = 0 after the propagation to z = hz
   const float r0 = acc_res(hp[0], s.x), r1 = acc_res(hp[1], s.y);
-  acc_add(s.x, float(K[0][0] * U(r0) + K[0][1] * U(r1)));
-  acc_add(s.y, float(K[1][0] * U(r0) + K[1][1] * U(r1)));
+  acc_update(s.x, hp[0], r0, float(K[0][0] * U(r0) + K[0][1] * U(r1)));
+  acc_update(s.y, hp[1], r1, float(K[1][0] * U(r0) + K[1][1] * U(r1)));
   s.ipt = float(U(s.ipt) + (K[2][0] * U(r0) + K[2][1] * U(r1)));
-  acc_add(s.phi, float(K[3][0] * U(r0) + K[3][1] * U(r1)));
-  s.theta = float(U(s.theta) + (K[4][0] * U(r0) + K[4][1] * U(r1)));
+  const float dphi = float(K[3][0] * U(r0) + K[3][1] * U(r1));
+  const float theta_new = float(U(s.theta) + (K[4][0] * U(r0) + K[4][1] * U(r1)));
+  const float dth = theta_new - s.theta;
+  acc_add(s.phi, dphi);
+  s.theta = theta_new;
+  rotate(s.cP, s.sP, dphi);
+  rotate(s.cT, s.sT, dth);
   // Joseph form: P = (I - K H) C, C'' = P - P H^T K^T + K V K^T, with
   // P(i,j) = C(i,j) - K(i,0) C(0,j) - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0.
   const U Cm[5][5] = {{C00, C10, C30, C40, C50},

@@ -185,9 +185,12 @@ def test_known_answer_validation_block(p2z, ctx, kat_seed, mode):
         want = {"x": f["avgx"], "y": f["avgy"], "z": f["avgz"], "dx": f["avgdx"], "dy": f["avgdy"], "pt": f["avgpt"],
                 "phi": f["avgphi"], "theta": f["avgtheta"]}
         want = {k: float(v_) for k, v_ in want.items()}
-    # printed with 6 decimals: the last printed digit may differ by 1
+    # printed with 6 decimals: the last printed digit may differ by 1.  The
+    # precise form's means may also differ from the FP64 ones by 5e-7 relative
+    # (the golden log's FP32 evaluation is 1.6e-5 off in pt).
+    rel = 0.0 if mode == "reference_rounding" else 5e-7
     for k in got:
-        assert abs(got[k] - want[k]) <= 1.5e-6, (mode, k, got[k], want[k])
+        assert abs(got[k] - want[k]) <= 1.5e-6 + rel * abs(want[k]), (mode, k, got[k], want[k])
 
 
 # ---------------------------------------------------------------------------
