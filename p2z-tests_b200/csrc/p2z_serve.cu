@@ -403,7 +403,7 @@ p2z_status p2z_server_submit(p2z_server *s, const void *trk_in, const void *hits
   r.mask = hit_mask;
   r.trk_out = trk_out;
   r.ntrks = ntrks;
-  r.nb = std::max<int64_t>(nb, 1);  // an empty event still takes one (all-padding) batch
+  r.nb = nb;
   r.info.ntrks = ntrks;
   const uint32_t all = s->cfg.nlayer >= 32 ? 0xffffffffu : ((1u << s->cfg.nlayer) - 1u);
   if (hit_mask) {
@@ -418,6 +418,14 @@ p2z_status p2z_server_submit(p2z_server *s, const void *trk_in, const void *hits
     r.id = s->next_id++;
     r.info.submit_s = now_s(s->t0);
     *id = r.id;
+    if (nb == 0) {
+      // an event without tracks has nothing to copy or compute: done at once
+      r.st = St::Done;
+      r.info.admit_s = r.info.launch_s = r.info.done_s = r.info.submit_s;
+      r.info.status = P2Z_OK;
+      s->reqs.emplace(r.id, r);
+      return P2Z_OK;
+    }
     s->reqs.emplace(r.id, r);
     s->pending.push_back(r.id);
   }
@@ -439,16 +447,23 @@ p2z_status p2z_server_poll(p2z_server *s, int64_t id, p2z_request_info *info) {
 p2z_status p2z_server_wait(p2z_server *s, int64_t id, double timeout_s, p2z_request_info *info) {
   if (!s) return P2Z_BAD_ARG;
   std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->reqs.find(id);
-  if (it == s->reqs.end()) return P2Z_BAD_ARG;
   const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
-  while (it->second.st != St::Done) {
-    if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && it->second.st != St::Done)
-      return P2Z_TIMEOUT;
+  for (;;) {
+    // look the request up after every wake-up: submits from other threads may
+    // have rehashed the table meanwhile
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return P2Z_BAD_ARG;
+    if (it->second.st == St::Done) {
+      if (info) *info = it->second.info;
+      s->reqs.erase(it);  // a completed request is released once reported
+      return P2Z_OK;
+    }
+    if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+      auto again = s->reqs.find(id);
+      if (again == s->reqs.end()) return P2Z_BAD_ARG;
+      if (again->second.st != St::Done) return P2Z_TIMEOUT;
+    }
   }
-  if (info) *info = it->second.info;
-  s->reqs.erase(it);  // a completed request is released once reported
-  return P2Z_OK;
 }
 
 p2z_status p2z_server_replay(p2z_server *s, int64_t nreq, const void *const *trk_in, const void *const *hits,
