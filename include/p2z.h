@@ -201,6 +201,32 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
 p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *d_trk, const void *d_hits,
                            int nlayer, int layer, int what, int update, float kfact);
 
+/* The same pass as p2z_run_device with the persistent schedule, for callers
+ * that cannot allocate device memory: applications whose device memory belongs
+ * to another allocator that must account for every byte (a framework's caching
+ * allocator, an experiment's memory manager with fixed budgets), and
+ * latency-critical paths on which cudaMalloc/cudaFree are not allowed because
+ * they can synchronise the whole device.  No counterpart in the reference.
+ * It needs no p2z_context (creating one allocates) and calls no allocating
+ * routine: its scratch -- the work counter, the status word and, for uneven
+ * events given without a hit mask, the padding mask and event offsets -- is a
+ * fixed array of about 5 MB inside the library, which every GPU that loads the
+ * library holds until the process exits.  Limits: an uneven run without a hit
+ * mask may have at most P2Z_NOALLOC_MAX_SLOTS track slots and
+ * P2Z_NOALLOC_MAX_EVENTS events (larger runs return P2Z_BAD_ARG with a message
+ * in p2z_last_error(NULL)); uniform runs and runs with a caller-provided mask
+ * have no size limit.  Enqueued on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream) on the current device; returns after enqueueing.
+ * The first call on a device looks up the scratch array's device address (once
+ * per device, with that device current); make that first call before any
+ * stream capture.  All calls share the one scratch array and each call resets
+ * what must start at zero, so calls whose work overlaps on the GPU (different
+ * streams, or concurrent host threads) race on it: serialise them. */
+#define P2Z_NOALLOC_MAX_SLOTS (1 << 20)
+#define P2Z_NOALLOC_MAX_EVENTS (1 << 16)
+p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
+                                  const uint32_t *d_hit_mask, void *d_trk_out, void *stream);
+
 /* ---- inputs (prepareTracks / prepareHits) ----------------------------------- */
 
 /* Seed structs, layout-identical to the reference's ATRK and AHIT

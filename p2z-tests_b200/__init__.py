@@ -142,6 +142,7 @@ _SIGS = {
     "p2z_sizeof_mphit": (C.c_size_t, [C.c_int]),
     "p2z_run": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, _VP, C.POINTER(Stats)]),
     "p2z_run_device": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP, C.POINTER(Stats)]),
+    "p2z_run_device_noalloc": (C.c_int, [C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP]),
     "p2z_step_device": (C.c_int, [_VP, C.c_int, C.c_int64, _VP, _CVP, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_float]),
     "p2z_prepare": (C.c_int, [C.POINTER(Atrk), C.POINTER(Ahit), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int,
@@ -189,6 +190,8 @@ def declared_symbols() -> list[str]:
     """Function names declared in include/p2z.h (parsed from the header)."""
     import re
     text = INCLUDE_H.read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)  # comments are not declarations
+    text = re.sub(r"//[^\n]*", " ", text)
     return sorted(set(re.findall(r"\b(p2z_[a-z0-9_]+)\s*\(", text)))
 
 

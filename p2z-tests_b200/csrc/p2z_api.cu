@@ -346,6 +346,11 @@ p2z_status count_updates(p2z_context *ctx, const Plan &pl, const uint32_t *d_mas
 
 }  // namespace
 
+namespace p2z {
+// Records the message p2z_last_error(NULL) returns (failures with no context).
+void set_context_free_error(const char *msg) { fail(nullptr, P2Z_OK, "%s", msg); }
+}  // namespace p2z
+
 extern "C" {
 
 const char *p2z_status_string(p2z_status s) {
