@@ -167,6 +167,61 @@ def uneven_counts(n_events, seed):
 
 
 # ---------------------------------------------------------------------------
+# serving
+# ---------------------------------------------------------------------------
+
+SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
+
+
+def run_serving(p2z, device, rank, args):
+    """Events of 1k-20k tracks (log-uniform), 20 layers with missing-hit masks
+    (5-20 hits, 10% dropped), the 3x3 update with its FP64 inversion island,
+    admitted under a 40 GB ring; Poisson arrivals at each swept rate."""
+    rng = np.random.default_rng(1234 + rank)
+    npool = 128
+    counts = np.exp(rng.uniform(np.log(1000), np.log(20000), npool)).astype(np.int64)
+    pool = []
+    for i, n in enumerate(counts):
+        cfg = p2z.make_config(bsize=32, nevts=1, event_ntrks=[int(n)], nlayer=20)
+        nb = p2z.num_batches(cfg)
+        t = p2z.PinnedArray((nb, 28, 32))
+        h = p2z.PinnedArray((nb, 20, 9, 32))
+        m = p2z.PinnedArray((nb * 32,), np.uint32)
+        o = p2z.PinnedArray((nb, 28, 32))
+        p2z.generate_physics(cfg, p2z.physics_params(seed=5000 + i, nthreads=0), with_mask=True,
+                             out=(t.array, h.array, m.array))
+        p2z.mask_layers(m.array, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=77 + i)
+        pool.append((t, h, m, o, int(n)))
+    out = {"workload": "events of 1k-20k tracks (log-uniform), 20 layers, 5-20 hits/track with 10% dropped, "
+                       "3x3 update with FP64 inversion + Joseph, Poisson arrivals",
+           "device_budget_gb": 40, "events_per_rate": args.serve_events, "rates": []}
+    with p2z.Server(device=device, bsize=32, nlayer=20, update="3x3_f64", budget_bytes=40 << 30,
+                    max_inflight=2) as srv:
+        # warm-up
+        srv.replay([(e[0].array, e[1].array, e[2].array, e[4], e[3].array) for e in pool[:16]],
+                   np.zeros(16))
+        for rate in SERVE_RATES:
+            n = args.serve_events
+            idx = rng.integers(0, npool, n)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+            evs = [(pool[i][0].array, pool[i][1].array, pool[i][2].array, pool[i][4], pool[i][3].array) for i in idx]
+            infos = srv.replay(evs, arrivals)
+            lat = np.array([x.done_s - x.submit_s for x in infos]) * 1e3
+            span = max(x.done_s for x in infos) - min(x.submit_s for x in infos)
+            upd = sum(x.updates for x in infos)
+            out["rates"].append({
+                "offered_events_per_s": rate, "events": n,
+                "achieved_events_per_s": n / span, "updates_per_s": upd / span,
+                "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+                "latency_ms_max": float(lat.max()),
+                "mean_group_events": float(np.mean([x.group_events for x in infos]))})
+    for e in pool:
+        for a in e[:4]:
+            a.free()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
 
@@ -243,6 +298,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-events", type=int, default=1500)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -363,6 +420,11 @@ def main():
                "ratio": res["persistent"] / res["per_event"]}
         del udt, udh, udo, udm
 
+    # serving: continuous batching under Poisson arrivals
+    serving = None
+    if not args.no_serving:
+        serving = run_serving(p2z, local, rank, args)
+
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -396,6 +458,7 @@ def main():
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,
         "batched_vs_plain": bvp,
+        "serving": serving,
         "outputs_finite": out_ok,
     }
     if not args.no_cpu_baseline:

@@ -19,6 +19,20 @@
 
 #include "p2z_math.cuh"
 
+// Register budget: at most P2Z_MAX_CTA_THREADS threads per CTA and at least
+// P2Z_MIN_CTAS such CTAs resident per SM (1 leaves the register count to
+// ptxas).  Hit prefetch depth: how many layers ahead the hits are requested
+// (1 or 2) in the all-layers loop.
+#ifndef P2Z_MAX_CTA_THREADS
+#define P2Z_MAX_CTA_THREADS 256
+#endif
+#ifndef P2Z_MIN_CTAS
+#define P2Z_MIN_CTAS 1
+#endif
+#ifndef P2Z_PREFETCH_DEPTH
+#define P2Z_PREFETCH_DEPTH 1
+#endif
+
 namespace p2z {
 
 constexpr int TRK_WORDS = 28;  // 6 par + 21 cov + 1 q
@@ -172,7 +186,29 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
 
   bool singular = false;
   HitRegs<NH> h0, h1;
-  if constexpr (!MASKED) {
+  if constexpr (!MASKED && P2Z_PREFETCH_DEPTH >= 2) {
+    // every layer present; three hit buffers rotate so that the hits of the
+    // next two layers are in flight during a step
+    const int64_t stride = (int64_t)HIT_WORDS * B;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
+    const int nl = a.nlayer;
+    HitRegs<NH> h2;
+    load_hit<B, NH>(h0, hp);
+    if (nl > 1) load_hit<B, NH>(h1, hp + stride);
+    if (nl > 2) load_hit<B, NH>(h2, hp + 2 * stride);
+    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    int l = 1;
+    for (; l + 2 < nl; l += 3) {  // layers l, l+1, l+2 are in h1, h2 and (after the load) h0
+      if (l + 2 < nl) load_hit<B, NH>(h0, hp + (l + 2) * stride);
+      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      if (l + 3 < nl) load_hit<B, NH>(h1, hp + (l + 3) * stride);
+      singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
+      if (l + 4 < nl) load_hit<B, NH>(h2, hp + (l + 4) * stride);
+      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+    }
+    if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+    if (l + 1 < nl) singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
+  } else if constexpr (!MASKED) {
     // every layer present: counted loop, hits addressed by a running pointer;
     // two hit buffers alternate so the next layer is in flight during a step
     const int64_t stride = (int64_t)HIT_WORDS * B;
@@ -223,15 +259,11 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   if (singular) atomicOr(a.status, 1u);
 }
 
-// Register budget: at most 256 threads per CTA and at least P2Z_MIN_CTAS
-// 256-thread CTAs resident per SM (1 leaves the register count to ptxas).
-#ifndef P2Z_MIN_CTAS
-#define P2Z_MIN_CTAS 1
-#endif
+
 
 // One launch over slots [slot_begin, slot_end), one thread per slot.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(256, P2Z_MIN_CTAS) k_flat(RunArgs a) {
+__global__ void __launch_bounds__(P2Z_MAX_CTA_THREADS, P2Z_MIN_CTAS) k_flat(RunArgs a) {
   const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= a.slot_end) return;
   process_slot<B, UPD, SC, MASKED>(a, slot);
@@ -242,7 +274,7 @@ __global__ void __launch_bounds__(256, P2Z_MIN_CTAS) k_flat(RunArgs a) {
 // the range is exhausted.  Work items are taken in slot order, so concurrently
 // running warps read neighbouring batches.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(256, P2Z_MIN_CTAS) k_persistent(RunArgs a) {
+__global__ void __launch_bounds__(P2Z_MAX_CTA_THREADS, P2Z_MIN_CTAS) k_persistent(RunArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t nslots = a.slot_end - a.slot_begin;
   const unsigned long long nitems = (unsigned long long)((nslots + 31) / 32);

@@ -125,21 +125,30 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // ---------------------------------------------------------------------------
 // sin / cos / versine
 // ---------------------------------------------------------------------------
-// Taylor series about 0 for |a| <= 0.5: sin(a) = a - a^3/3! + ... + a^9/9!
-// (truncation < a^11/11! ~ 1.2e-11 relative) and the versine
-// 1 - cos(a) = a^2/2! - a^4/4! + ... - a^10/10! (truncation < a^12/12!).
-// The coefficients are (-1)^n/(2n+1)! and (-1)^n/(2n)!, rounded to float.
+// Taylor series about 0 for |a| <= 0.5: sin(a) = a - a^3/3! + a^5/5! - a^7/7!
+// (truncation below a^9/9! ~ 5.4e-9 |a| at |a| = 0.5) and the versine
+// 1 - cos(a) = a^2/2! - a^4/4! + a^6/6! - a^8/8! (truncation below
+// a^10/10! ~ 2.2e-9 of the versine at |a| = 0.5).  The coefficients are
+// (-1)^n/(2n+1)! and (-1)^n/(2n)!, rounded to float.
 __device__ __forceinline__ void sv_series(float a, float *s, float *v) {
   const float a2 = a * a;
-  float ps = fmaf(a2, 2.7557319e-6f, -1.9841270e-4f);
-  ps = fmaf(a2, ps, 8.3333333e-3f);
+  float ps = fmaf(a2, -1.9841270e-4f, 8.3333333e-3f);
   ps = fmaf(a2, ps, -1.6666667e-1f);
   *s = fmaf(a * a2, ps, a);
-  float pv = fmaf(a2, 2.7557319e-7f, -2.4801587e-5f);
-  pv = fmaf(a2, pv, 1.3888889e-3f);
-  pv = fmaf(a2, pv, -4.1666667e-2f);
-  pv = fmaf(a2, pv, 0.5f);
+  float pv = fmaf(a2, 2.4801587e-5f, -1.3888889e-3f);
+  pv = fmaf(a2, pv, 4.1666667e-2f);
+  pv = fmaf(a2, -pv, 0.5f);
   *v = a2 * pv;
+}
+
+// The same for the small Kalman corrections of phi and theta, to a^5/5! and
+// a^6/6! (truncation below 1e-9 relative for |a| <= 0.2, 1.6e-6 at |a| = 0.5).
+__device__ __forceinline__ void sv_series_short(float a, float *s, float *v) {
+  const float a2 = a * a;
+  const float ps = fmaf(a2, 8.3333333e-3f, -1.6666667e-1f);
+  *s = fmaf(a * a2, ps, a);
+  const float pv = fmaf(a2, 1.3888889e-3f, -4.1666667e-2f);
+  *v = a2 * fmaf(a2, pv, 0.5f);
 }
 
 // sin(a) and 1 - cos(a) without cancellation.
@@ -170,13 +179,12 @@ __device__ __forceinline__ float cosf_cr(float x) { return (float)cos((double)x)
 
 // Rotate the unit vector (c, s) = (cos t, sin t) to t + d:
 // cos(t+d) = c - (c*v + s*w), sin(t+d) = s - (s*v - c*w) with w = sin d and
-// v = 1 - cos d from their series (sv_series; truncation below 1e-11 for
-// |d| <= 0.5 and below 3e-8 for |d| <= 1).  No branch: Kalman corrections to
-// phi and theta are far below 1 rad for any track the filter can follow, and
-// NaN or Inf propagate.
+// v = 1 - cos d from their short series (sv_series_short).  No branch: Kalman
+// corrections to phi and theta are far below 0.2 rad for any track the filter
+// can follow, and NaN or Inf propagate.
 __device__ __forceinline__ void rotate(float &c, float &s, float d) {
   float w, v;
-  sv_series(d, &w, &v);
+  sv_series_short(d, &w, &v);
   const float cn = c - fmaf(c, v, s * w);
   const float sn = s - fmaf(s, v, -(c * w));
   c = cn;
