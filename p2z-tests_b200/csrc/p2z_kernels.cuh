@@ -19,16 +19,9 @@
 
 #include "p2z_math.cuh"
 
-// Register budget: at most P2Z_MAX_CTA_THREADS threads per CTA and at least
-// P2Z_MIN_CTAS such CTAs resident per SM (1 leaves the register count to
-// ptxas).  Hit prefetch depth: how many layers ahead the hits are requested
-// (1 or 2) in the all-layers loop.
-#ifndef P2Z_MAX_CTA_THREADS
-#define P2Z_MAX_CTA_THREADS 256
-#endif
-#ifndef P2Z_MIN_CTAS
-#define P2Z_MIN_CTAS 1
-#endif
+// Hit prefetch depth in the all-layers loop: how many layers ahead the hits
+// are requested (0: at the start of each step; 1 or 2: before the step that
+// precedes them, so their latency overlaps the arithmetic).
 #ifndef P2Z_PREFETCH_DEPTH
 #define P2Z_PREFETCH_DEPTH 1
 #endif
@@ -62,6 +55,11 @@ struct Types {
       typename std::conditional<UPD == UPDK_V2_REF, float,
                                 typename std::conditional<UPD == UPDK_V2_COMP, DF, AP>::type>::type>::type;
   static constexpr int NH = (UPD == UPDK_3X3_F64 || UPD == UPDK_3X3_COMP) ? 9 : 6;
+  // Register budget: kernels allow up to 256 threads per CTA and ask ptxas
+  // for MIN_CTAS such CTAs per SM.  For the 2-D FP32 kinds, 3 caps them at 80
+  // registers (24 resident warps per SM), which measured faster than the 88
+  // ptxas picks unconstrained; 1 leaves the count to ptxas.
+  static constexpr int MIN_CTAS = (UPD == UPDK_V2 || UPD == UPDK_V2_COMP) ? 3 : 1;
 };
 
 struct RunArgs {
@@ -117,13 +115,13 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
   Jac<T> J;
   if constexpr (UPD == UPDK_F64) {
     hx = propagate_params_f64(s, zout, k);
-    J = jacobian_precise<double>(hx, k, s.ipt);
+    J = jacobian_precise<double, GENERAL>(hx, k, s.ipt);
   } else if constexpr (UPD == UPDK_V2_REF) {
     hx = propagate_params_ref(s, zout, k);
     J = jacobian_ref(hx, k, s.ipt);
   } else {
     hx = propagate_params_precise<SC>(s, zout, k, ik);
-    J = jacobian_precise<float>(hx, k, s.ipt);
+    J = jacobian_precise<float, GENERAL>(hx, k, s.ipt);
   }
   if constexpr (GENERAL) propagate_cov_general(s, b21, hx, J);
   else propagate_cov_reduced(s, J);
@@ -208,6 +206,17 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
     }
     if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
     if (l + 1 < nl) singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
+  } else if constexpr (!MASKED && P2Z_PREFETCH_DEPTH == 0) {
+    // every layer present, one hit buffer: each layer's hits are loaded at the
+    // start of its step (latency hidden by other warps only)
+    const int64_t stride = (int64_t)HIT_WORDS * B;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
+    load_hit<B, NH>(h0, hp);
+    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    for (int l = 1; l < a.nlayer; ++l) {
+      load_hit<B, NH>(h0, hp + l * stride);
+      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+    }
   } else if constexpr (!MASKED) {
     // every layer present: counted loop, hits addressed by a running pointer;
     // two hit buffers alternate so the next layer is in flight during a step
@@ -263,7 +272,7 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
 
 // One launch over slots [slot_begin, slot_end), one thread per slot.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(P2Z_MAX_CTA_THREADS, P2Z_MIN_CTAS) k_flat(RunArgs a) {
+__global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_flat(RunArgs a) {
   const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= a.slot_end) return;
   process_slot<B, UPD, SC, MASKED>(a, slot);
@@ -274,7 +283,7 @@ __global__ void __launch_bounds__(P2Z_MAX_CTA_THREADS, P2Z_MIN_CTAS) k_flat(RunA
 // the range is exhausted.  Work items are taken in slot order, so concurrently
 // running warps read neighbouring batches.
 template <int B, int UPD, int SC, bool MASKED>
-__global__ void __launch_bounds__(P2Z_MAX_CTA_THREADS, P2Z_MIN_CTAS) k_persistent(RunArgs a) {
+__global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t nslots = a.slot_end - a.slot_begin;
   const unsigned long long nitems = (unsigned long long)((nslots + 31) / 32);

@@ -225,9 +225,14 @@ struct Trk {
 
 // Helix quantities shared by the parameter update and the Jacobian.  omc and
 // omcC are 1 - cos(alpha) and 1 - cos(cosP*sin(alpha)).
+//   FORM_PRECISE / FP64 fields: tanT = tan(theta), icT2 = 1/cos^2(theta),
+//     dzk = deltaZ/k, kpt = k*pt, m1 = cosP*sina, m2 = sinP*sina.
+//   FORM_REFERENCE fields: sinT, icosT, icosTk (the reference's own scalars).
 template <typename T>
 struct Helix {
-  T deltaZ, pt, cosP, sinP, sinT, icosT, icosTk, sina, cosa, omc, sCPs, omcC;
+  T deltaZ, pt, cosP, sinP, sina, cosa, omc, sCPs, omcC;
+  T tanT, icT2, dzk, kpt, m1, m2;
+  T sinT, icosT, icosTk;
 };
 
 // The Jacobian entries that act on a covariance with zero z row (reference
@@ -237,12 +242,21 @@ struct Jac {
   T a3, a4, a5;    // J(0,3) J(0,4) J(0,5)
   T a9, a10, a11;  // J(1,3) J(1,4) J(1,5)
   T a27, a29;      // J(4,3) J(4,5)
+  T a2, a8, a26;   // J(0,2) J(1,2) J(4,2): first layer only
 };
 
 // ---- FORM_PRECISE -----------------------------------------------------------
 
-// Parameter propagation (reference :627-647).  With SC_FAST, icosT/k is taken
-// as icosT * (1/k): one rounding more than the reference's division.
+// Parameter propagation (reference :627-647), with the reference's products
+// regrouped around shared factors (exact in real arithmetic):
+//   alpha = deltaZ*sinT*ipt*icosT/k = (deltaZ/k)*tanT*ipt,
+//   x += k*(pxin*sina - pyin*(1-cosa)) = k*pt*(cosP*sina - sinP*omc),
+//   y += k*(pyin*sina + pxin*(1-cosa)) = k*pt*(sinP*sina + cosP*omc).
+// With SC_FAST, deltaZ/k is taken as deltaZ * (1/k): one rounding more than a
+// division.  sin and 1 - cos of cosP*sina, used only by the Jacobian, come from
+// the series of sv_series with no range branch: |cosP*sina| <= 1, where the
+// series' truncation is below 3.3e-6 relative (sin) and 6.1e-7 (versine) --
+// far inside what the covariance needs -- and below 1e-8 for |a| <= 0.5.
 template <int SC, typename A>
 __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
   Helix<float> h;
@@ -250,22 +264,25 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   h.pt = rcp_nr(s.ipt);
   h.cosP = s.cP;
   h.sinP = s.sP;
-  h.sinT = s.sT;
-  const float pxin = h.cosP * h.pt;
-  const float pyin = h.sinP * h.pt;
-  h.icosT = rcp_nr(s.cT);
-  h.icosTk = (SC == SC_FAST) ? h.icosT * ik : __fdiv_rn(h.icosT, k);
-  const float alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
+  const float icosT = rcp_nr(s.cT);
+  h.tanT = s.sT * icosT;
+  h.icT2 = icosT * icosT;
+  h.dzk = (SC == SC_FAST) ? h.deltaZ * ik : __fdiv_rn(h.deltaZ, k);
+  const float alpha = (h.dzk * h.tanT) * s.ipt;
   sin_versine<SC>(alpha, &h.sina, &h.omc);
   h.cosa = 1.f - h.omc;
-  acc_add(s.x, k * (pxin * h.sina - pyin * h.omc));
-  acc_add(s.y, k * (pyin * h.sina + pxin * h.omc));
+  h.kpt = k * h.pt;
+  h.m1 = h.cosP * h.sina;
+  h.m2 = h.sinP * h.sina;
+  acc_add(s.x, h.kpt * fmaf(-h.sinP, h.omc, h.m1));
+  acc_add(s.y, h.kpt * fmaf(h.cosP, h.omc, h.m2));
   s.z = zout;
   acc_add(s.phi, alpha);
-  sin_versine<SC>(h.cosP * h.sina, &h.sCPs, &h.omcC);
+  if (SC == SC_FAST) sv_series(h.m1, &h.sCPs, &h.omcC);
+  else sin_versine<SC>(h.m1, &h.sCPs, &h.omcC);
   // phi advanced by alpha: rotate (cos phi, sin phi) with sin(alpha) and the versine
-  s.cP = h.cosP - fmaf(h.cosP, h.omc, h.sinP * h.sina);
-  s.sP = h.sinP - fmaf(h.sinP, h.omc, -(h.cosP * h.sina));
+  s.cP = h.cosP - fmaf(h.cosP, h.omc, h.m2);
+  s.sP = h.sinP - fmaf(h.sinP, h.omc, -h.m1);
   return h;
 }
 
@@ -276,35 +293,45 @@ __device__ __forceinline__ void init_direction(Trk<float, A> &s) {
   sincosf(s.theta, &s.sT, &s.cT);
 }
 
-// The same entries with the shared factors taken out (exact in real
-// arithmetic; fewer products):
+// The Jacobian entries (reference :655-666) with the shared factors taken out
+// (exact in real arithmetic; fewer products):
 //   B = 1 - sinP*sC,  D = cosP^2*sC + sinP,  u = cosP*dZ*cosa*B,  v = dZ*cosa*D,
-//   J03 = u*sinT*icosT*pt - k*pt^2*(cosP*sina - sinP*omcC)   J05 = u*icosT^2
-//   J13 = v*sinT*icosT*pt - k*pt^2*(sinP*sina + cosP*omcC)   J15 = v*icosT^2
-//   J04 = -k*pt*(sinP*sina*B + cosP*omcC)                     J14 = k*pt*(cosP*sina*B - sinP*omcC)
-template <typename T>
+//   J03 = u*tanT*pt - k*pt^2*(cosP*sina - sinP*omcC)   J05 = u/cosT^2
+//   J13 = v*tanT*pt - k*pt^2*(sinP*sina + cosP*omcC)   J15 = v/cosT^2
+//   J04 = -k*pt*(sinP*sina*B + cosP*omcC)               J14 = k*pt*(cosP*sina*B - sinP*omcC)
+//   J43 = (dZ/k)*tanT                                   J45 = (dZ/k)*ipt/cosT^2
+// and, for the first layer, J02 = -cosP*tanT*cosa*B, J12 = cosa*tanT*(cosP^2*sC - sinP),
+// J42 = -ipt*tanT/k.
+template <typename T, bool GENERAL = false>
 __device__ __forceinline__ Jac<T> jacobian_precise(const Helix<T> &h, T k, T ipt) {
   Jac<T> J;
-  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT;
+  const T cosP = h.cosP, sinP = h.sinP;
   const T dzc = h.deltaZ * h.cosa;
   const T B = T(1) - sinP * h.sCPs;
-  const T D = cosP * cosP * h.sCPs + sinP;
-  const T icT2 = h.icosT * h.icosT;
-  const T stp = sinT * (h.icosT * h.pt);
-  const T kpt = k * h.pt;
+  const T cc = cosP * cosP * h.sCPs;
+  const T D = cc + sinP;
+  const T stp = h.tanT * h.pt;
+  const T kpt = h.kpt;
   const T kpt2 = kpt * h.pt;
-  const T m1 = cosP * h.sina, m2 = sinP * h.sina;
+  const T m1 = h.m1, m2 = h.m2;
   const T n1 = cosP * h.omcC, n2 = sinP * h.omcC;
   const T u = cosP * dzc * B;
   const T v = dzc * D;
   J.a3 = u * stp - kpt2 * (m1 - n2);
-  J.a5 = u * icT2;
+  J.a5 = u * h.icT2;
   J.a9 = v * stp - kpt2 * (m2 + n1);
-  J.a11 = v * icT2;
+  J.a11 = v * h.icT2;
   J.a4 = -kpt * (m2 * B + n1);
   J.a10 = kpt * (m1 * B - n2);
-  J.a27 = sinT * h.deltaZ * h.icosTk;
-  J.a29 = ipt * h.deltaZ * (h.icosT * h.icosTk);
+  J.a27 = h.dzk * h.tanT;
+  J.a29 = (h.dzk * ipt) * h.icT2;
+  if constexpr (GENERAL) {
+    J.a2 = -(cosP * h.tanT) * (h.cosa * B);
+    J.a8 = h.cosa * h.tanT * (cc - sinP);
+    J.a26 = -(ipt * h.tanT) / k;
+  } else {
+    J.a2 = J.a8 = J.a26 = T(0);
+  }
   return J;
 }
 
@@ -354,6 +381,10 @@ __device__ __forceinline__ Jac<float> jacobian_ref(const Helix<float> &h, float 
   J.a11 = deltaZ * cosa * (cosP * cosP * sCosPsina + sinP) * (icosT * icosT);
   J.a27 = sinT * deltaZ * (icosTk);
   J.a29 = ipt * deltaZ * (icosT * icosTk);
+  // column 2 (first layer): reference :655, :659, :663
+  J.a2 = cosP * sinT * (sinP * cosa * sCosPsina - cosa) * icosT;
+  J.a8 = cosa * sinT * (cosP * cosP * sCosPsina - sinP) * icosT;
+  J.a26 = -ipt * sinT * (icosTk);
   return J;
 }
 
@@ -363,21 +394,24 @@ __device__ __forceinline__ Helix<double> propagate_params_f64(Trk<double, double
   Helix<double> h;
   h.deltaZ = zout - s.z;
   h.pt = 1.0 / s.ipt;
-  double cosT;
+  double cosT, sinT;
   sincos(s.phi, &h.sinP, &h.cosP);
-  sincos(s.theta, &h.sinT, &cosT);
-  const double pxin = h.cosP * h.pt, pyin = h.sinP * h.pt;
-  h.icosT = 1.0 / cosT;
-  h.icosTk = h.icosT / k;
-  const double alpha = h.deltaZ * h.sinT * s.ipt * h.icosTk;
+  sincos(s.theta, &sinT, &cosT);
+  h.tanT = sinT / cosT;
+  h.icT2 = 1.0 / (cosT * cosT);
+  h.dzk = h.deltaZ / k;
+  const double alpha = h.dzk * h.tanT * s.ipt;
   sincos(alpha, &h.sina, &h.cosa);
   h.omc = 1.0 - h.cosa;
-  s.x += k * (pxin * h.sina - pyin * h.omc);
-  s.y += k * (pyin * h.sina + pxin * h.omc);
+  h.kpt = k * h.pt;
+  h.m1 = h.cosP * h.sina;
+  h.m2 = h.sinP * h.sina;
+  s.x += h.kpt * (h.m1 - h.sinP * h.omc);
+  s.y += h.kpt * (h.m2 + h.cosP * h.omc);
   s.z = zout;
   s.phi += alpha;
   double cC;
-  sincos(h.cosP * h.sina, &h.sCPs, &cC);
+  sincos(h.m1, &h.sCPs, &cC);
   h.omcC = 1.0 - cC;
   return h;
 }
@@ -427,14 +461,13 @@ __device__ __forceinline__ void propagate_cov_reduced(Trk<T, A> &s, const Jac<T>
 
 // General form on the full 21-element input covariance b[] (the first
 // propagation of a track), including the Jacobian's z column a2 = J(0,2),
-// a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663).
+// a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663), which the Jacobian
+// functions fill for the first layer.
 template <typename T, typename A>
 __device__ __forceinline__ void propagate_cov_general(Trk<T, A> &s, const T (&b)[21], const Helix<T> &h,
                                                       const Jac<T> &J) {
-  const T cosP = h.cosP, sinP = h.sinP, sinT = h.sinT, cosa = h.cosa;
-  const T a2 = cosP * sinT * (sinP * cosa * h.sCPs - cosa) * h.icosT;
-  const T a8 = cosa * sinT * (cosP * cosP * h.sCPs - sinP) * h.icosT;
-  const T a26 = -s.ipt * sinT * h.icosTk;
+  (void)h;
+  const T a2 = J.a2, a8 = J.a8, a26 = J.a26;
   const T a3 = J.a3, a4 = J.a4, a5 = J.a5, a9 = J.a9, a10 = J.a10, a11 = J.a11, a27 = J.a27, a29 = J.a29;
   const T t0 = b[0] + a2 * b[3] + a3 * b[6] + a4 * b[10] + a5 * b[15];
   const T t2 = b[3] + a2 * b[5] + a3 * b[8] + a4 * b[12] + a5 * b[17];
