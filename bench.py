@@ -13,7 +13,12 @@ tracks x 20 layers.  Inputs (8.1 GB) are larger than L2, so no flush is needed.
           and device->host copies inside the timed region
   batched_vs_plain  uneven events (2000 events, log-normal track counts,
           5-20 hits per track with 10% of layers dropped): the persistent
-          work-queue kernel replayed as a CUDA graph vs one launch per event
+          work-queue kernel replayed as a CUDA graph vs one launch per event,
+          each with the block size the autotuner measured best for it
+  autotune  p2z_autotune's sweep (bsize x AOSOA/SoA x schedule x block size)
+          on the headline and the uneven workloads; the headline step runs
+          the reference's layout (bsize 32 AOSOA) with the schedule and block
+          size the sweep found best for that layout
 
 `--impl reference` times the reference's own CPU hot loop (its OpenMP source
 compiled unchanged into oracle/_ref) on this host's cores, on the same
@@ -173,6 +178,22 @@ def uneven_counts(n_events, seed):
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
 
+def tune_summary(best, rows, wall_s):
+    """Compact report of an autotune sweep: the fastest row overall, per bsize,
+    per layout and per schedule, and the row the reference's layout gets."""
+    def fastest(pred):
+        sel = [r for r in rows if pred(r)]
+        return min(sel, key=lambda r: r["ms"]) if sel else None
+    out = {"configurations": len(rows), "sweep_wall_s": wall_s, "best": best,
+           "best_bsize32_aosoa": fastest(lambda r: r["bsize"] == 32 and r["layout"] == "aosoa")}
+    for key in ("bsize", "layout", "schedule"):
+        vals = sorted({r[key] for r in rows}, key=str)
+        out[f"best_per_{key}"] = {str(v): {"ms": fastest(lambda r: r[key] == v)["ms"],
+                                           "updates_per_s": fastest(lambda r: r[key] == v)["updates_per_s"]}
+                                  for v in vals}
+    return out
+
+
 def run_serving(p2z, device, rank, args):
     """Events of 1k-20k tracks (log-uniform), 20 layers with missing-hit masks
     (5-20 hits, 10% dropped), the 3x3 update with its FP64 inversion island,
@@ -300,6 +321,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-events", type=int, default=1500)
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -316,7 +338,8 @@ def main():
     stream = torch.cuda.Stream()
 
     nev = args.nevts
-    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat")
+    # schedule and block size left open: the context applies what p2z_autotune measured
+    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20)
     params = p2z.physics_params(seed=20240601 + rank)
     trk, hit = p2z.generate_physics(cfg, params)
     updates = nev * 9600 * 20
@@ -329,6 +352,12 @@ def main():
                                     p2z.C.c_void_p(stream.cuda_stream), None)
         if rc != p2z.OK:
             raise p2z.P2zError(rc, p2z.lib.p2z_last_error(ctx.h).decode())
+
+    tune_head = None
+    if not args.no_tune:
+        t0 = time.time()
+        best, rows = ctx.autotune(cfg, dt, dh, reps=3)
+        tune_head = tune_summary(best, rows, time.time() - t0)
 
     for _ in range(args.warmup):
         step()
@@ -395,9 +424,19 @@ def main():
         udt, udh = torch.from_numpy(ut).cuda(), torch.from_numpy(uh).cuda()
         udo = torch.empty_like(udt)
         udm = torch.from_numpy(um.view(np.int32)).cuda()
-        res = {}
+        res, blocks = {}, {"persistent": 128, "per_event": 128}
+        tune_uneven = None
+        if not args.no_tune:
+            t0 = time.time()
+            best, rows = ctx.autotune(ucfg, udt, udh, d_mask=udm, reps=3)
+            tune_uneven = tune_summary(best, rows, time.time() - t0)
+            for sched in blocks:
+                r = min((r for r in rows if r["bsize"] == 32 and r["layout"] == "aosoa" and r["schedule"] == sched),
+                        key=lambda r: r["ms"])
+                blocks[sched] = r["block_threads"]
         for sched in ("persistent", "per_event"):
-            c = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=sched)
+            c = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=sched,
+                                block_threads=blocks[sched])
             for _ in range(3):
                 p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), udt.data_ptr(), udh.data_ptr(), udm.data_ptr(),
                                        udo.data_ptr(), p2z.C.c_void_p(stream.cuda_stream), None)
@@ -417,7 +456,8 @@ def main():
                            "5-20 hits/track, 10% layers dropped",
                "tracks": int(counts.sum()), "updates_per_step": u_upd,
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
-               "ratio": res["persistent"] / res["per_event"]}
+               "ratio": res["persistent"] / res["per_event"], "block_threads": blocks,
+               "autotune": tune_uneven}
         del udt, udh, udo, udm
 
     # serving: continuous batching under Poisson arrivals
@@ -444,7 +484,9 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
                    "updates_per_step_per_gpu": updates, "l2": "inputs 8.1 GB > L2, no flush",
-                   "parallelism": f"dp{world} (independent event shards)"},
+                   "parallelism": f"dp{world} (independent event shards)",
+                   "launch": ({k: tune_head["best_bsize32_aosoa"][k] for k in ("schedule", "block_threads")}
+                              if tune_head else {"schedule": "flat", "block_threads": 128})},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": (tpu * updates / launches_per_step) if tpu else None,
@@ -455,6 +497,7 @@ def main():
                           "peak_source": f"148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (nominal, no measured "
                                          f"FP32 peak on this pool)"},
         "clocks": clk,
+        "autotune": tune_head,
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,
         "batched_vs_plain": bvp,

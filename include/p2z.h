@@ -30,6 +30,13 @@
  *   entirely (neither propagated to nor updated with).  Padding slots carry
  *   mask 0 and are copied through unchanged.
  *
+ * SoA layout (p2z_config.layout = P2Z_LAYOUT_SOA; no counterpart in the
+ * reference): the same slots (slot = batch*B + t, events padded to multiples of
+ * bsize as above) stored as one batch spanning all nslots = nbatches*bsize
+ * slots: tracks as float[28][nslots] (element p of slot s at p*nslots + s) and
+ * hits as float[nlayer][9][nslots] (element p of layer l at
+ * (l*9 + p)*nslots + s).  Masks are indexed by slot in both layouts.
+ *
  * Threading: a p2z_context belongs to one host thread at a time.  Device-side
  * work is ordered on the stream passed in (or the context's own stream).
  */
@@ -94,6 +101,12 @@ typedef enum p2z_schedule {
   P2Z_SCHED_PERSISTENT = 3
 } p2z_schedule;
 
+/* Array layouts (see the top of this file). */
+typedef enum p2z_layout {
+  P2Z_LAYOUT_AOSOA = 0, /* the reference's MPTRK / MPHIT batches */
+  P2Z_LAYOUT_SOA = 1    /* one array per element over all slots */
+} p2z_layout;
+
 /* Flags */
 #define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan inputs for NaN/Inf first -> P2Z_NONFINITE_INPUT */
 #define P2Z_FLAG_STRICT       0x2u  /* return P2Z_SINGULAR if any det <= 0 was met */
@@ -123,10 +136,13 @@ typedef struct p2z_config {
                             recomputes the outputs from the inputs; 0 is treated as 1 */
   float kfact;           /* 0 -> P2Z_KFACT_DEFAULT */
   int32_t update;        /* p2z_update_kind */
-  int32_t schedule;      /* p2z_schedule */
-  int32_t block_threads; /* threads per CTA; 0 -> tuned default */
+  int32_t schedule;      /* p2z_schedule; AUTO -> the schedule p2z_autotune measured best on
+                            this context for the same key, else the rule under p2z_schedule */
+  int32_t block_threads; /* threads per CTA, a multiple of 32 in 32..256; 0 -> the value
+                            p2z_autotune measured best on this context for the same update,
+                            flags, bsize, layout and masking, else 128 */
   uint32_t flags;        /* P2Z_FLAG_* */
-  int32_t reserved0;
+  int32_t layout;        /* p2z_layout of the track, hit and output arrays */
   /* Uneven form (optional, host memory): nevts track counts.  NULL -> uniform. */
   const int64_t *event_ntrks;
 } p2z_config;
@@ -215,7 +231,8 @@ p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *
  * mask may have at most P2Z_NOALLOC_MAX_SLOTS track slots and
  * P2Z_NOALLOC_MAX_EVENTS events (larger runs return P2Z_BAD_ARG with a message
  * in p2z_last_error(NULL)); uniform runs and runs with a caller-provided mask
- * have no size limit.  Enqueued on `stream` (a cudaStream_t; NULL is the
+ * have no size limit.  AOSOA layout only (P2Z_UNSUPPORTED otherwise).
+ * Enqueued on `stream` (a cudaStream_t; NULL is the
  * legacy default stream) on the current device; returns after enqueueing.
  * The first call on a device looks up the scratch array's device address (once
  * per device, with that device current); make that first call before any
@@ -226,6 +243,48 @@ p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *
 #define P2Z_NOALLOC_MAX_EVENTS (1 << 16)
 p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
                                   const uint32_t *d_hit_mask, void *d_trk_out, void *stream);
+
+/* ---- layouts and tuning (no counterpart in the reference) ------------------ */
+
+/* Copy tracks, hits and (optionally) masks of the same events from the layout
+ * and bsize `from` describes to those `to` describes, on the device, enqueued
+ * on `stream` (NULL = the context's stream).  from and to must describe the
+ * same events: equal nevts and nlayer and the same track count per event
+ * (uniform ntrks or event_ntrks).  Padding slots of the destination get zero
+ * tracks and hits and, when masks are converted, mask 0.  Pass both masks or
+ * neither.  Destination buffers must not overlap the sources. */
+p2z_status p2z_relayout_device(p2z_context *ctx, const p2z_config *from, const p2z_config *to,
+                               const void *d_trk_in, const void *d_hits_in, const uint32_t *d_mask_in,
+                               void *d_trk_out, void *d_hits_out, uint32_t *d_mask_out, void *stream);
+
+/* One measured launch configuration. */
+typedef struct p2z_tune_entry {
+  int32_t bsize;          /* 8, 16, 32, 64 */
+  int32_t layout;         /* p2z_layout */
+  int32_t schedule;       /* P2Z_SCHED_FLAT, _PER_EVENT or _PERSISTENT */
+  int32_t block_threads;  /* 32 .. 256 */
+  double ms;              /* mean device time of one pass */
+  double updates_per_s;   /* present-hit updates per second */
+} p2z_tune_entry;
+
+/* Autotuner: measures one pass of cfg's work (its update kind and flags, one
+ * iteration) on the caller's device data under every combination of bsize
+ * {8,16,32,64} x layout {AOSOA, SOA} x schedule {FLAT, PERSISTENT, and
+ * PER_EVENT when nevts <= 4096} x block_threads {32,64,128,256}, each the mean
+ * of `reps` passes (0 -> 3) after one warm-up pass.  The inputs are converted
+ * to each candidate's bsize and layout with p2z_relayout_device into scratch
+ * buffers the call allocates and frees (about twice the input size); the
+ * caller's buffers are only read.  Results: the number of configurations
+ * measured in *n_entries, the first max_entries of them in `entries` (may be
+ * NULL when max_entries is 0), the fastest in *best.
+ * Side effect: for every (bsize, layout) measured, the context remembers the
+ * fastest schedule and block size, and later runs with block_threads = 0 or
+ * schedule = AUTO and the same update, flags, bsize, layout and masking use
+ * them.  A different bsize or layout is a different data layout, which only
+ * the caller can adopt (p2z_relayout_device).  Synchronous. */
+p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
+                        const uint32_t *d_hit_mask, int reps, p2z_tune_entry *entries, int max_entries,
+                        int *n_entries, p2z_tune_entry *best);
 
 /* ---- inputs (prepareTracks / prepareHits) ----------------------------------- */
 

@@ -40,6 +40,11 @@ UPDATE_NAMES = {"v2": UPDATE_V2, "v2_comp": UPDATE_V2_COMP, "3x3_f64": UPDATE_3X
 SCHED_AUTO, SCHED_FLAT, SCHED_PER_EVENT, SCHED_PERSISTENT = range(4)
 SCHED_NAMES = {"auto": SCHED_AUTO, "flat": SCHED_FLAT, "per_event": SCHED_PER_EVENT,
                "persistent": SCHED_PERSISTENT}
+SCHED_LABELS = {v: k for k, v in SCHED_NAMES.items()}
+# array layouts
+LAYOUT_AOSOA, LAYOUT_SOA = 0, 1
+LAYOUT_NAMES = {"aosoa": LAYOUT_AOSOA, "soa": LAYOUT_SOA}
+LAYOUT_LABELS = {v: k for k, v in LAYOUT_NAMES.items()}
 # flags
 FLAG_CHECK_INPUTS = 0x1
 FLAG_STRICT = 0x2
@@ -60,7 +65,7 @@ class Config(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("bsize", C.c_int32), ("nevts", C.c_int64), ("ntrks", C.c_int64),
                 ("nlayer", C.c_int32), ("niter", C.c_int32), ("kfact", C.c_float), ("update", C.c_int32),
                 ("schedule", C.c_int32), ("block_threads", C.c_int32), ("flags", C.c_uint32),
-                ("reserved0", C.c_int32), ("event_ntrks", C.POINTER(C.c_int64))]
+                ("layout", C.c_int32), ("event_ntrks", C.POINTER(C.c_int64))]
 
 
 class Stats(C.Structure):
@@ -112,6 +117,17 @@ class ValidationPartial(C.Structure):
         p.sq[:] = [float(x) for x in a[9:15]]
         p.nnans, p.nfail, p.ngood = (int(round(x)) for x in a[15:18])
         return p
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("bsize", C.c_int32), ("layout", C.c_int32), ("schedule", C.c_int32), ("block_threads", C.c_int32),
+                ("ms", C.c_double), ("updates_per_s", C.c_double)]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["layout"] = LAYOUT_LABELS.get(d["layout"], d["layout"])
+        d["schedule"] = SCHED_LABELS.get(d["schedule"], d["schedule"])
+        return d
 
 
 class ServerConfig(C.Structure):
@@ -167,6 +183,10 @@ _SIGS = {
     "p2z_server_replay": (C.c_int, [_VP, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                     C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.POINTER(C.c_void_p),
                                     C.POINTER(C.c_double), C.POINTER(RequestInfo)]),
+    "p2z_relayout_device": (C.c_int, [_VP, C.POINTER(Config), C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP, _VP,
+                                      _VP]),
+    "p2z_autotune": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, C.c_int, C.POINTER(TuneEntry), C.c_int,
+                               C.POINTER(C.c_int), C.POINTER(TuneEntry)]),
     "p2z_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
     "p2z_host_free": (C.c_int, [_VP]),
 }
@@ -236,6 +256,30 @@ def tracks_to_aos(trk: np.ndarray) -> dict:
     return {"par": t[:, :6].copy(), "cov": t[:, 6:27].copy(), "q": t[:, 27].copy().view(np.int32)}
 
 
+def tracks_to_soa(trk: np.ndarray) -> np.ndarray:
+    """(nbatches, 28, B) AOSOA -> (28, nslots) SoA (P2Z_LAYOUT_SOA), same slot order."""
+    nb, w, B = trk.shape
+    return np.ascontiguousarray(trk.transpose(1, 0, 2)).reshape(w, nb * B)
+
+
+def hits_to_soa(hits: np.ndarray) -> np.ndarray:
+    """(nbatches, nlayer, 9, B) AOSOA -> (nlayer, 9, nslots) SoA."""
+    nb, nl, w, B = hits.shape
+    return np.ascontiguousarray(hits.transpose(1, 2, 0, 3)).reshape(nl, w, nb * B)
+
+
+def tracks_from_soa(trk: np.ndarray, bsize: int) -> np.ndarray:
+    """(28, nslots) SoA -> (nslots/bsize, 28, bsize) AOSOA."""
+    w, ns = trk.shape
+    return np.ascontiguousarray(trk.reshape(w, ns // bsize, bsize).transpose(1, 0, 2))
+
+
+def hits_from_soa(hits: np.ndarray, bsize: int) -> np.ndarray:
+    """(nlayer, 9, nslots) SoA -> (nslots/bsize, nlayer, 9, bsize) AOSOA."""
+    nl, w, ns = hits.shape
+    return np.ascontiguousarray(hits.reshape(nl, w, ns // bsize, bsize).transpose(2, 0, 1, 3))
+
+
 def hits_to_aos(hits: np.ndarray) -> dict:
     """(nbatches, nlayer, 9, B) -> pos (nslots, nlayer, 3), cov (nslots, nlayer, 6)."""
     nb, nl, w, B = hits.shape
@@ -244,7 +288,7 @@ def hits_to_aos(hits: np.ndarray) -> dict:
 
 
 def make_config(bsize=32, nevts=1, ntrks=None, nlayer=20, niter=1, kfact=0.0, update=UPDATE_V2,
-                schedule=SCHED_AUTO, block_threads=0, flags=0, event_ntrks=None):
+                schedule=SCHED_AUTO, block_threads=0, flags=0, event_ntrks=None, layout=LAYOUT_AOSOA):
     cfg = Config()
     cfg.abi_version = ABI_VERSION
     cfg.bsize = bsize
@@ -257,6 +301,7 @@ def make_config(bsize=32, nevts=1, ntrks=None, nlayer=20, niter=1, kfact=0.0, up
     cfg.schedule = SCHED_NAMES.get(schedule, schedule) if isinstance(schedule, str) else schedule
     cfg.block_threads = block_threads
     cfg.flags = flags
+    cfg.layout = LAYOUT_NAMES.get(layout, layout) if isinstance(layout, str) else layout
     if event_ntrks is not None:
         arr = np.ascontiguousarray(event_ntrks, dtype=np.int64)
         cfg._event_ntrks_keep = arr  # keep alive with the struct
@@ -438,6 +483,24 @@ class Context:
     def step_device(self, bsize, nbatches, d_trk, d_hits, nlayer, layer, what=3, update=UPDATE_V2, kfact=0.0):
         _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
                                    kfact), self.h)
+
+    def relayout_device(self, cfg_from: Config, cfg_to: Config, d_trk_in, d_hits_in, d_trk_out, d_hits_out,
+                        d_mask_in=None, d_mask_out=None, stream=None):
+        """Convert device arrays between bsizes / AOSOA / SoA (p2z_relayout_device)."""
+        _check(lib.p2z_relayout_device(self.h, C.byref(cfg_from), C.byref(cfg_to), _ptr(d_trk_in), _ptr(d_hits_in),
+                                       _ptr(d_mask_in), _ptr(d_trk_out), _ptr(d_hits_out), _ptr(d_mask_out),
+                                       stream), self.h)
+
+    def autotune(self, cfg: Config, d_trk_in, d_hits, d_mask=None, reps=3, max_entries=256):
+        """Measure every bsize x layout x schedule x block size (p2z_autotune).
+        Returns (best, entries) as dicts, entries sorted by time."""
+        rows = (TuneEntry * max_entries)()
+        n = C.c_int(0)
+        best = TuneEntry()
+        _check(lib.p2z_autotune(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits), _ptr(d_mask), reps, rows,
+                                max_entries, C.byref(n), C.byref(best)), self.h)
+        entries = sorted((rows[i].as_dict() for i in range(min(n.value, max_entries))), key=lambda d: d["ms"])
+        return best.as_dict(), entries
 
 
 class Server:

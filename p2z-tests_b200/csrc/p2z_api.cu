@@ -34,8 +34,15 @@ struct DevBuf {
 struct GraphKey {
   RunArgs args;
   int bsize, upd, sc, block, grid;
-  bool masked;
+  bool masked, soa;
   bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+};
+
+// Launch shape p2z_autotune measured fastest for one kind of run.
+struct Tuned {
+  int upd, sc, B;
+  bool soa, masked;
+  int block, schedule;
 };
 
 }  // namespace
@@ -53,6 +60,7 @@ struct p2z_context {
   bool has_graph = false;
   GraphKey gkey;
   cudaGraphExec_t gexec = nullptr;
+  std::vector<Tuned> tuned;                 // p2z_autotune results
   std::string last_error;
 };
 
@@ -112,6 +120,7 @@ struct Plan {
   int64_t nbatches = 0;
   int64_t nslots = 0;
   bool uneven = false;
+  bool soa = false;          // P2Z_LAYOUT_SOA
   std::vector<int64_t> ev_slot_begin;  // nevts + 1 entries
   std::vector<uint8_t> batch_valid;    // uneven: real lanes per batch
 };
@@ -129,6 +138,9 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
     return fail(ctx, P2Z_BAD_ARG, "schedule %d unknown", cfg->schedule);
   if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
     return fail(ctx, P2Z_BAD_ARG, "block_threads %d not a multiple of 32 in 32..256", cfg->block_threads);
+  if (cfg->layout != P2Z_LAYOUT_AOSOA && cfg->layout != P2Z_LAYOUT_SOA)
+    return fail(ctx, P2Z_BAD_ARG, "layout %d unknown", cfg->layout);
+  pl.soa = cfg->layout == P2Z_LAYOUT_SOA;
   pl.B = cfg->bsize;
   pl.nlayer = cfg->nlayer;
   pl.niter = cfg->niter > 0 ? cfg->niter : 1;
@@ -221,6 +233,8 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   spec.args = base;
   spec.args.queue = queue;
   spec.bsize = pl.B;
+  spec.soa = pl.soa;
+  spec.args.ws = pl.nslots;
   spec.upd = pl.upd;
   spec.sc = pl.sc;
   spec.masked = base.mask != nullptr;
@@ -273,6 +287,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   key.block = spec.block;
   key.grid = spec.grid;
   key.masked = spec.masked;
+  key.soa = spec.soa;
   if (!(ctx->has_graph && ctx->gkey == key)) {
     if (ctx->gexec) {
       cudaGraphExecDestroy(ctx->gexec);
@@ -301,9 +316,21 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   return P2Z_OK;
 }
 
-int resolve_schedule(const Plan &pl, bool masked) {
+// Applies the autotuner's measurement for this kind of run to the fields the
+// caller left open (block_threads = 0, schedule = AUTO), then resolves AUTO.
+int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool masked) {
+  masked = masked || pl.uneven;
+  if (ctx) {
+    for (const Tuned &t : ctx->tuned) {
+      if (t.upd == pl.upd && t.sc == pl.sc && t.B == pl.B && t.soa == pl.soa && t.masked == masked) {
+        if (cfg->block_threads == 0) pl.block = t.block;
+        if (pl.schedule == P2Z_SCHED_AUTO) pl.schedule = t.schedule;
+        break;
+      }
+    }
+  }
   if (pl.schedule != P2Z_SCHED_AUTO) return pl.schedule;
-  return (pl.uneven || masked) ? P2Z_SCHED_PERSISTENT : P2Z_SCHED_FLAT;
+  return masked ? P2Z_SCHED_PERSISTENT : P2Z_SCHED_FLAT;
 }
 
 // Builds the padding mask of uneven events into ctx->valid / ctx->mask.
@@ -344,11 +371,60 @@ p2z_status count_updates(p2z_context *ctx, const Plan &pl, const uint32_t *d_mas
   return P2Z_OK;
 }
 
+// p2z_run, SoA layout: host->device copy of slots [s0, s0 + n) of every
+// element row of the tracks (28 rows) and hits (nlayer x 9 rows, or the first
+// 6 of each layer's 9 when `six`), with pitched copies.
+p2z_status copy_soa_chunk(p2z_context *ctx, const Plan &pl, const void *trk_in, const void *hits, int64_t s0, int64_t n,
+                          bool six, cudaStream_t st, int64_t *h2d) {
+  const size_t pitch = (size_t)pl.nslots * 4, off = (size_t)s0 * 4, w = (size_t)n * 4;
+  P2Z_CUDA(ctx, cudaMemcpy2DAsync((char *)ctx->trk.p + off, pitch, (const char *)trk_in + off, pitch, w, TRK_WORDS,
+                                  cudaMemcpyHostToDevice, st));
+  *h2d += (int64_t)(w * TRK_WORDS);
+  if (!six) {
+    P2Z_CUDA(ctx, cudaMemcpy2DAsync((char *)ctx->hits.p + off, pitch, (const char *)hits + off, pitch, w,
+                                    (size_t)HIT_WORDS * pl.nlayer, cudaMemcpyHostToDevice, st));
+    *h2d += (int64_t)(w * HIT_WORDS * pl.nlayer);
+    return P2Z_OK;
+  }
+  // rows (l, e) for e < 6 of each layer: a 3-D box of the [nlayer][9][nslots] array
+  cudaMemcpy3DParms c;
+  std::memset(&c, 0, sizeof c);
+  c.srcPtr = make_cudaPitchedPtr(const_cast<void *>(hits), pitch, pitch, HIT_WORDS);
+  c.dstPtr = make_cudaPitchedPtr(ctx->hits.p, pitch, pitch, HIT_WORDS);
+  c.srcPos = make_cudaPos(off, 0, 0);
+  c.dstPos = make_cudaPos(off, 0, 0);
+  c.extent = make_cudaExtent(w, 6, (size_t)pl.nlayer);
+  c.kind = cudaMemcpyHostToDevice;
+  P2Z_CUDA(ctx, cudaMemcpy3DAsync(&c, st));
+  *h2d += (int64_t)(w * 6 * pl.nlayer);
+  return P2Z_OK;
+}
+
 }  // namespace
 
 namespace p2z {
 // Records the message p2z_last_error(NULL) returns (failures with no context).
 void set_context_free_error(const char *msg) { fail(nullptr, P2Z_OK, "%s", msg); }
+
+// Autotuner hooks: the context's device and stream, its error message, and
+// the record of a measured best launch shape for the runs cfg describes.
+int context_device(const p2z_context *ctx) { return ctx->device; }
+cudaStream_t context_stream(const p2z_context *ctx) { return ctx->stream; }
+p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg) { return fail(ctx, st, "%s", msg); }
+p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule) {
+  Plan pl;
+  p2z_status r = make_plan(ctx, cfg, pl);
+  if (r != P2Z_OK) return r;
+  Tuned t{pl.upd, pl.sc, pl.B, pl.soa, masked || pl.uneven, block, schedule};
+  for (Tuned &o : ctx->tuned) {
+    if (o.upd == t.upd && o.sc == t.sc && o.B == t.B && o.soa == t.soa && o.masked == t.masked) {
+      o = t;
+      return P2Z_OK;
+    }
+  }
+  ctx->tuned.push_back(t);
+  return P2Z_OK;
+}
 }  // namespace p2z
 
 extern "C" {
@@ -475,7 +551,7 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
   base.nlayer = pl.nlayer;
   base.kfact = pl.kfact;
   base.status = ctx->d_status;
-  const int schedule = resolve_schedule(pl, mask != nullptr);
+  const int schedule = resolve_schedule(ctx, pl, cfg, mask != nullptr);
   int launches = 0;
   if (stats) {
     P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
@@ -545,7 +621,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
   base.nlayer = pl.nlayer;
   base.kfact = pl.kfact;
   base.status = ctx->d_status;
-  int schedule = resolve_schedule(pl, d_mask != nullptr);
+  int schedule = resolve_schedule(ctx, pl, cfg, d_mask != nullptr);
   // The per-event form is timed as it stands: copies first, then one launch per event.
   const bool per_event = schedule == P2Z_SCHED_PER_EVENT;
   // Only the 2-D updates read just the first 6 of the 9 hit words.
@@ -564,6 +640,11 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
       const int64_t b0 = c * cb, b1 = std::min(pl.nbatches, b0 + cb);
       if (b1 <= b0) continue;
       const int64_t nbc = b1 - b0;
+      if (pl.soa) {
+        // slots [b0*B, b1*B) of every element row: pitched copies
+        r = copy_soa_chunk(ctx, pl, trk_in, hits, b0 * pl.B, nbc * pl.B, six, st, &h2d);
+        if (r != P2Z_OK) return r;
+      } else {
       P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->trk.p + b0 * tb, (const char *)trk_in + b0 * tb, nbc * tb,
                                     cudaMemcpyHostToDevice, st));
       h2d += nbc * tb;
@@ -579,6 +660,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
                                       cudaMemcpyHostToDevice, st));
         h2d += (int64_t)(hrow * hrows);
       }
+      }
       if (user_mask) {
         P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->mask.p + b0 * pl.B * 4, (const char *)hit_mask + b0 * pl.B * 4,
                                       nbc * pl.B * 4, cudaMemcpyHostToDevice, st));
@@ -588,8 +670,14 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
         r = enqueue_pass(ctx, pl, base, b0 * pl.B, b1 * pl.B, schedule == P2Z_SCHED_PERSISTENT ? P2Z_SCHED_FLAT : schedule,
                          st, ctx->d_queue + (c & 1), &launches);
         if (r != P2Z_OK) return r;
-        P2Z_CUDA(ctx, cudaMemcpyAsync((char *)trk_out + b0 * tb, (const char *)ctx->out.p + b0 * tb, nbc * tb,
-                                      cudaMemcpyDeviceToHost, st));
+        if (pl.soa) {
+          const size_t pitch = (size_t)pl.nslots * 4, off = (size_t)b0 * pl.B * 4, w = (size_t)nbc * pl.B * 4;
+          P2Z_CUDA(ctx, cudaMemcpy2DAsync((char *)trk_out + off, pitch, (const char *)ctx->out.p + off, pitch, w,
+                                          TRK_WORDS, cudaMemcpyDeviceToHost, st));
+        } else {
+          P2Z_CUDA(ctx, cudaMemcpyAsync((char *)trk_out + b0 * tb, (const char *)ctx->out.p + b0 * tb, nbc * tb,
+                                        cudaMemcpyDeviceToHost, st));
+        }
         d2h += nbc * tb;
       }
     }

@@ -72,21 +72,33 @@ struct RunArgs {
   float kfact;
   unsigned int *status;            // bit 0: a det <= 0 was met
   unsigned long long *queue;       // persistent kernels: next work item
+  int64_t ws;                      // SoA layout (B == 0): slots in the arrays = word stride
 };
 
+// Layouts.  B > 0: the reference's AOSOA batches of width B (element e of a
+// lane at e*B from the lane's first word).  B == 0: SoA -- one batch as wide as
+// the whole array of ws slots: tracks [28][ws], hits [nlayer][9][ws].
 template <int B>
 __device__ __forceinline__ const float *trk_lane(const float *base, int64_t slot) {
-  const int64_t b = slot / B;
-  const int t = (int)(slot % B);
-  return base + b * (int64_t)(TRK_WORDS * B) + t;
+  if constexpr (B == 0) {
+    return base + slot;
+  } else {
+    const int64_t b = slot / B;
+    const int t = (int)(slot % B);
+    return base + b * (int64_t)(TRK_WORDS * B) + t;
+  }
 }
 
 // Hit words of slot's batch on layer l: &pos.data[t], stride B per element.
 template <int B>
-__device__ __forceinline__ const float *hit_lane(const float *hits, int64_t slot, int nlayer, int l) {
-  const int64_t b = slot / B;
-  const int t = (int)(slot % B);
-  return hits + (b * nlayer + l) * (int64_t)(HIT_WORDS * B) + t;
+__device__ __forceinline__ const float *hit_lane(const float *hits, int64_t slot, int nlayer, int l, int64_t ws) {
+  if constexpr (B == 0) {
+    return hits + (int64_t)l * HIT_WORDS * ws + slot;
+  } else {
+    const int64_t b = slot / B;
+    const int t = (int)(slot % B);
+    return hits + (b * nlayer + l) * (int64_t)(HIT_WORDS * B) + t;
+  }
 }
 
 // Hit words a kernel needs: x, y, z, V00, V10, V11 and, for the 3-D update,
@@ -96,11 +108,11 @@ struct HitRegs {
   float w[NH];
 };
 
-template <int B, int NH>
-__device__ __forceinline__ void load_hit(HitRegs<NH> &h, const float *p) {
-  // pos[0..2] then cov[0..NH-4]; element e of the lane at p[e*B]
+template <int NH>
+__device__ __forceinline__ void load_hit(HitRegs<NH> &h, const float *p, int64_t ws) {
+  // pos[0..2] then cov[0..NH-4]; element e of the lane at p[e*ws]
 #pragma unroll
-  for (int e = 0; e < NH; ++e) h.w[e] = __ldg(p + e * B);
+  for (int e = 0; e < NH; ++e) h.w[e] = __ldg(p + e * ws);
 }
 
 // One propagate + update step.  GENERAL: first present layer (full 21-element
@@ -151,6 +163,7 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   using T = typename Types<UPD>::T;
   using A = typename Types<UPD>::A;
   constexpr int NH = Types<UPD>::NH;
+  const int64_t WS = (B > 0) ? (int64_t)B : a.ws;  // word stride
   const float *tin = trk_lane<B>(a.trk, slot);
   float *tout = const_cast<float *>(trk_lane<B>(a.out, slot));
 
@@ -159,11 +172,11 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
 
   float in[TRK_WORDS];
 #pragma unroll
-  for (int e = 0; e < TRK_WORDS; ++e) in[e] = __ldg(tin + e * B);
+  for (int e = 0; e < TRK_WORDS; ++e) in[e] = __ldg(tin + e * WS);
 
   if (m == 0u) {  // no hits (or a padding slot): the track passes through
 #pragma unroll
-    for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, in[e]);
+    for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, in[e]);
     return;
   }
 
@@ -187,21 +200,21 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   if constexpr (!MASKED && P2Z_PREFETCH_DEPTH >= 2) {
     // every layer present; three hit buffers rotate so that the hits of the
     // next two layers are in flight during a step
-    const int64_t stride = (int64_t)HIT_WORDS * B;
-    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
+    const int64_t stride = HIT_WORDS * WS;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0, WS);
     const int nl = a.nlayer;
     HitRegs<NH> h2;
-    load_hit<B, NH>(h0, hp);
-    if (nl > 1) load_hit<B, NH>(h1, hp + stride);
-    if (nl > 2) load_hit<B, NH>(h2, hp + 2 * stride);
+    load_hit<NH>(h0, hp, WS);
+    if (nl > 1) load_hit<NH>(h1, hp + stride, WS);
+    if (nl > 2) load_hit<NH>(h2, hp + 2 * stride, WS);
     singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
     int l = 1;
     for (; l + 2 < nl; l += 3) {  // layers l, l+1, l+2 are in h1, h2 and (after the load) h0
-      if (l + 2 < nl) load_hit<B, NH>(h0, hp + (l + 2) * stride);
+      if (l + 2 < nl) load_hit<NH>(h0, hp + (l + 2) * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
-      if (l + 3 < nl) load_hit<B, NH>(h1, hp + (l + 3) * stride);
+      if (l + 3 < nl) load_hit<NH>(h1, hp + (l + 3) * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
-      if (l + 4 < nl) load_hit<B, NH>(h2, hp + (l + 4) * stride);
+      if (l + 4 < nl) load_hit<NH>(h2, hp + (l + 4) * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
     }
     if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
@@ -209,44 +222,44 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   } else if constexpr (!MASKED && P2Z_PREFETCH_DEPTH == 0) {
     // every layer present, one hit buffer: each layer's hits are loaded at the
     // start of its step (latency hidden by other warps only)
-    const int64_t stride = (int64_t)HIT_WORDS * B;
-    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
-    load_hit<B, NH>(h0, hp);
+    const int64_t stride = HIT_WORDS * WS;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0, WS);
+    load_hit<NH>(h0, hp, WS);
     singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
     for (int l = 1; l < a.nlayer; ++l) {
-      load_hit<B, NH>(h0, hp + l * stride);
+      load_hit<NH>(h0, hp + l * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
     }
   } else if constexpr (!MASKED) {
     // every layer present: counted loop, hits addressed by a running pointer;
     // two hit buffers alternate so the next layer is in flight during a step
-    const int64_t stride = (int64_t)HIT_WORDS * B;
-    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0);
+    const int64_t stride = HIT_WORDS * WS;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0, WS);
     const int nl = a.nlayer;
-    load_hit<B, NH>(h0, hp);
-    if (nl > 1) load_hit<B, NH>(h1, hp + stride);
+    load_hit<NH>(h0, hp, WS);
+    if (nl > 1) load_hit<NH>(h1, hp + stride, WS);
     singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
     int l = 1;
     for (; l + 1 < nl; l += 2) {
-      load_hit<B, NH>(h0, hp + (l + 1) * stride);
+      load_hit<NH>(h0, hp + (l + 1) * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
-      if (l + 2 < nl) load_hit<B, NH>(h1, hp + (l + 2) * stride);
+      if (l + 2 < nl) load_hit<NH>(h1, hp + (l + 2) * stride, WS);
       singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
     }
     if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
   } else {
     // present layers in order: lowest set bit first
     uint32_t rest = m & (m - 1u);
-    load_hit<B, NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(m) - 1));
-    if (rest) load_hit<B, NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+    load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(m) - 1, WS), WS);
+    if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
     singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
     while (rest) {
       rest &= rest - 1u;  // h1 holds the layer just removed from rest
-      if (rest) load_hit<B, NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+      if (rest) load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
       singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
       if (!rest) break;
       rest &= rest - 1u;  // h0 holds the layer just removed
-      if (rest) load_hit<B, NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1));
+      if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
       singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
     }
   }
@@ -264,7 +277,7 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   c[20] = float(s.c55);
   o[27] = in[27];
 #pragma unroll
-  for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, o[e]);
+  for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, o[e]);
   if (singular) atomicOr(a.status, 1u);
 }
 
@@ -301,6 +314,7 @@ __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArg
 struct LaunchSpec {
   RunArgs args;
   int bsize;
+  bool soa;      // SoA layout (args.ws = slots in the arrays)
   int upd;       // UPDK_*
   int sc;        // SC_*
   bool masked;
@@ -343,6 +357,7 @@ struct Dispatch {
     return fn_m<B, SC_ACCURATE>(masked, kind);
   }
   static const void *select(const LaunchSpec &s) {
+    if (s.soa) return fn_sc<0>(s.sc, s.masked, s.kind);
     switch (s.bsize) {
       case 8: return fn_sc<8>(s.sc, s.masked, s.kind);
       case 16: return fn_sc<16>(s.sc, s.masked, s.kind);

@@ -133,6 +133,7 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
   if (cfg->abi_version != P2Z_ABI_VERSION) return fail(P2Z_BAD_ARG, "abi_version mismatch");
   const int B = cfg->bsize;
   if (!(B == 8 || B == 16 || B == 32 || B == 64)) return fail(P2Z_UNSUPPORTED, "bsize not in {8,16,32,64}");
+  if (cfg->layout != P2Z_LAYOUT_AOSOA) return fail(P2Z_UNSUPPORTED, "only the AOSOA layout is supported here");
   if (cfg->nlayer < 1 || cfg->nlayer > 32) return fail(P2Z_BAD_ARG, "nlayer not in 1..32");
   if (cfg->nevts < 0) return fail(P2Z_BAD_ARG, "nevts < 0");
   if (cfg->update < P2Z_UPDATE_V2 || cfg->update > P2Z_UPDATE_F64) return fail(P2Z_BAD_ARG, "unknown update kind");

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) k_step(float *trk, const float *hits, int
   const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= nslots) return;
   float *tp = const_cast<float *>(trk_lane<B>(trk, slot));
-  const float *hp = hit_lane<B>(hits, slot, nlayer, layer);
+  const float *hp = hit_lane<B>(hits, slot, nlayer, layer, B);
   float p[6], C[21];
 #pragma unroll
   for (int e = 0; e < 6; ++e) p[e] = tp[e * B];
