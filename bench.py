@@ -86,53 +86,105 @@ def profile_traffic_per_update():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 2 ms from a thread (the data nvidia-smi reports),
+    or nvidia-smi -lms 200 when NVML is unavailable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []       # (time, sm_mhz, reasons bitmask)
+        self.sm_max = None
+        self.power_w = []
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+        self._handle = None
+        self._proc = None
+        self._lines = []
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:
+            pass
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = self.cuda_index
+        if vis:
+            try:
+                idx = int(vis.split(",")[self.cuda_index])
+            except (ValueError, IndexError):
+                pass
+        return pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            threading.Thread(target=self._read, daemon=True).start()
+            self._handle = self._nvml_handle()
+            nv = self._nvml
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(self._handle, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            self._nvml = None
+        try:
+            fields = "clocks.sm,clocks.max.sm,clocks_event_reasons.active"
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.cuda_index}", f"--query-gpu={fields}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=lambda: self._lines.extend(l.strip() for l in self._proc.stdout),
+                             daemon=True).start()
         except OSError:
-            self.proc = None
+            self._proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if self.proc is not None:
-            self.proc.terminate()
+    def _poll(self):
+        nv, h = self._nvml, self._handle
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
             try:
-                self.proc.wait(timeout=5)
+                self.samples.append((time.perf_counter(), float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                     int(get_reasons(h))))
+                if len(self.samples) % 25 == 1:
+                    self.power_w.append(nv.nvmlDeviceGetPowerUsage(h) / 1000.0)
+            except Exception:
+                break
+            time.sleep(0.002)
+
+    def stop(self, t0=None, t1=None):
+        """Summary of the samples taken between host times t0 and t1 (the
+        timed region; all samples when not given)."""
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=2)
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                self._proc.kill()
+            for l in self._lines:
+                f = [x.strip() for x in l.split(",")]
+                try:
+                    self.sm_max = float(f[1])
+                    self.samples.append((None, float(f[0]), int(f[2], 16)))
+                except (ValueError, IndexError):
+                    continue
+        sel = [x for x in self.samples if x[0] is None or t0 is None or t0 <= x[0] <= t1]
+        sm = [a for _, a, _ in sel]
+        mask = 0
+        for _, _, r in sel:
+            mask |= r
+        reasons = sorted(n for n, bit in self.REASONS.items() if mask & bit)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.sm_max, "reasons": reasons,
+                "samples": len(sm), "source": "nvml" if self._nvml else "nvidia-smi",
+                "power_w_median": float(np.median(self.power_w)) if self.power_w else None}
 
 
 def dist_setup(n_gpus):
@@ -366,15 +418,17 @@ def main():
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    time.sleep(0.3)
+    time.sleep(0.05)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_begin = time.perf_counter()
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    t_end = time.perf_counter()
     ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
+    clk = clocks.stop(t_begin, t_end)
     barrier(world)
     ms_max = barrier_max(world, ms)
     ms_step = ms_max / args.steps

@@ -331,6 +331,17 @@ void p2z_physics_defaults(p2z_physics_params *p);
 p2z_status p2z_generate_physics(const p2z_physics_params *p, const p2z_config *cfg, void *trk_out, void *hits_out,
                                 uint32_t *hit_mask);
 
+/* The same physics sample generated on the device into device buffers (AOSOA
+ * layout): the same per-slot computation in the same double expressions, so
+ * the output equals p2z_generate_physics's except where CUDA's and the C
+ * library's log/exp/sin/cos/tan/atan round a double differently (a float
+ * output then differs by one unit in the last place; rare).  p->nthreads is
+ * ignored.  Enqueued on `stream` (NULL = the context's stream); returns when
+ * the generation is complete.  No counterpart in the reference, which prepares
+ * its inputs on the host (src/propagate-toz-test_OMP.cpp:243-293). */
+p2z_status p2z_generate_physics_device(p2z_context *ctx, const p2z_physics_params *p, const p2z_config *cfg,
+                                       void *d_trk_out, void *d_hits_out, uint32_t *d_hit_mask, void *stream);
+
 /* Drop layers from a hit mask (no counterpart in the reference): each real
  * track (mask != 0) keeps a contiguous run of L layers starting at layer 0 with
  * L uniform in [min_hits, max_hits], then loses each layer independently with
@@ -338,6 +349,10 @@ p2z_status p2z_generate_physics(const p2z_physics_params *p, const p2z_config *c
  * (seed, slot). */
 p2z_status p2z_mask_layers(uint32_t *hit_mask, int64_t nslots, int nlayer, int min_hits, int max_hits,
                            double drop_prob, uint64_t seed);
+/* The same on a device mask array (bit-identical to p2z_mask_layers: the draws
+ * use no library function), enqueued on `stream` (NULL = the context's). */
+p2z_status p2z_mask_layers_device(p2z_context *ctx, uint32_t *d_hit_mask, int64_t nslots, int nlayer, int min_hits,
+                                  int max_hits, double drop_prob, uint64_t seed, void *stream);
 
 /* ---- validation block ------------------------------------------------------- */
 
@@ -373,8 +388,32 @@ p2z_status p2z_validate_partial(const void *trk_out, int bsize, int64_t nevts, i
 void p2z_validate_means(const p2z_validation_partial *pass1, double means[6]);
 p2z_status p2z_validate_combine(const p2z_validation_partial *pass1, const p2z_validation_partial *pass2,
                                 p2z_validation *v);
+/* The same two passes over DEVICE-resident output tracks (AOSOA, bsize
+ * batches, nevts*ntrks tracks), reduced on the GPU: every track's values and
+ * selection are computed exactly as in p2z_validate (the same double
+ * expressions, so the same counts); the sums are taken in a fixed tree order
+ * (deterministic from run to run) instead of the reference's sequential one,
+ * so they agree with the host's to about 1e-15 relative.  The per-block
+ * partials live in the context's scratch.  Enqueued on `stream` (NULL = the
+ * context's stream); returns when the results are on the host.  Replaces the
+ * host loop of the reference's validation block (:758-864) for outputs that
+ * are still on the device; p2z_validate_partial_device is the per-shard form. */
+p2z_status p2z_validate_device(p2z_context *ctx, const void *d_trk_out, int bsize, int64_t nevts, int64_t ntrks,
+                               const float hit_last[3], p2z_validation *v, void *stream);
+p2z_status p2z_validate_partial_device(p2z_context *ctx, const void *d_trk_out, int bsize, int64_t nevts,
+                                       int64_t ntrks, const float hit_last[3], const double means[6],
+                                       p2z_validation_partial *acc, void *stream);
 /* Print it with the reference's exact format (:866-876) to stdout. */
 void p2z_print_validation(const p2z_validation *v);
+/* The per-track dump of the reference's DUMP_OUTPUT build
+ * (src/propagate-toz-test_CUDA_v4.cu:1012-1143): for every track that passes
+ * the validation's NaN test and window (as in p2z_validate), one "%f" line
+ * with its output x, y, z in output_x.txt, output_y.txt, output_z.txt and its
+ * input x, y, z in input_x.txt, input_y.txt, input_z.txt, in the directory
+ * `dir` (NULL or "" = the current directory).  Host arrays.  The tracks are
+ * selected against the last-layer seed hit, as p2z_validate does. */
+p2z_status p2z_dump_tracks(const void *trk_in, const void *trk_out, int bsize, int64_t nevts, int64_t ntrks,
+                           const float hit_last[3], const char *dir);
 /* The machine-readable line of the reference (:756), parsed by its tools
  * (tools/compare.py:12): "formatted NITER nevts ntrks bsize nb wall 0 setup nthreads". */
 void p2z_print_formatted(int niter, int64_t nevts, int64_t ntrks, int bsize, double wall_s, double setup_s,

@@ -166,13 +166,21 @@ _SIGS = {
     "p2z_physics_defaults": (None, [C.POINTER(PhysicsParams)]),
     "p2z_generate_physics": (C.c_int, [C.POINTER(PhysicsParams), C.POINTER(Config), _VP, _VP, _VP]),
     "p2z_mask_layers": (C.c_int, [_VP, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64]),
+    "p2z_generate_physics_device": (C.c_int, [_VP, C.POINTER(PhysicsParams), C.POINTER(Config), _VP, _VP, _VP, _VP]),
+    "p2z_mask_layers_device": (C.c_int, [_VP, _VP, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64,
+                                         _VP]),
     "p2z_validate": (C.c_int, [_CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float), C.POINTER(Validation)]),
     "p2z_validate_partial": (C.c_int, [_CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float),
                                        C.POINTER(C.c_double), C.POINTER(ValidationPartial)]),
     "p2z_validate_means": (None, [C.POINTER(ValidationPartial), C.POINTER(C.c_double)]),
     "p2z_validate_combine": (C.c_int, [C.POINTER(ValidationPartial), C.POINTER(ValidationPartial),
                                        C.POINTER(Validation)]),
+    "p2z_validate_device": (C.c_int, [_VP, _CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float),
+                                      C.POINTER(Validation), _VP]),
+    "p2z_validate_partial_device": (C.c_int, [_VP, _CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float),
+                                              C.POINTER(C.c_double), C.POINTER(ValidationPartial), _VP]),
     "p2z_print_validation": (None, [C.POINTER(Validation)]),
+    "p2z_dump_tracks": (C.c_int, [_CVP, _CVP, C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_float), C.c_char_p]),
     "p2z_print_formatted": (None, [C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int]),
     "p2z_server_create": (C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "p2z_server_destroy": (C.c_int, [_VP]),
@@ -433,6 +441,13 @@ def shard_events(event_ntrks, world: int) -> list[tuple[int, int]]:
     return [(bounds[r], bounds[r + 1]) for r in range(world)]
 
 
+def dump_tracks(trk_in, trk_out, bsize, nevts, ntrks, hit_last, directory=None):
+    """The reference's DUMP_OUTPUT files (output_/input_ x, y, z .txt)."""
+    h = (C.c_float * 3)(*hit_last)
+    d = None if directory is None else str(directory).encode()
+    _check(lib.p2z_dump_tracks(_ptr(trk_in), _ptr(trk_out), bsize, nevts, ntrks, h, d))
+
+
 def print_validation(v: Validation):
     lib.p2z_print_validation(C.byref(v))
 
@@ -483,6 +498,32 @@ class Context:
     def step_device(self, bsize, nbatches, d_trk, d_hits, nlayer, layer, what=3, update=UPDATE_V2, kfact=0.0):
         _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
                                    kfact), self.h)
+
+    def generate_physics_device(self, cfg: Config, d_trk, d_hits, d_mask=None, params=None, stream=None):
+        """The physics sample generated on the device (p2z_generate_physics_device)."""
+        params = params or physics_params()
+        _check(lib.p2z_generate_physics_device(self.h, C.byref(params), C.byref(cfg), _ptr(d_trk), _ptr(d_hits),
+                                               _ptr(d_mask), stream), self.h)
+
+    def mask_layers_device(self, d_mask, nslots, nlayer, min_hits=5, max_hits=20, drop_prob=0.1, seed=7,
+                           stream=None):
+        _check(lib.p2z_mask_layers_device(self.h, _ptr(d_mask), nslots, nlayer, min_hits, max_hits, drop_prob,
+                                          seed, stream), self.h)
+
+    def validate_device(self, d_trk_out, bsize, nevts, ntrks, hit_last, stream=None) -> dict:
+        """The validation block reduced on the GPU (p2z_validate_device)."""
+        h = (C.c_float * 3)(*hit_last)
+        v = Validation()
+        _check(lib.p2z_validate_device(self.h, _ptr(d_trk_out), bsize, nevts, ntrks, h, C.byref(v), stream), self.h)
+        return v
+
+    def validate_partial_device(self, d_trk_out, bsize, nevts, ntrks, hit_last, means=None, stream=None):
+        h = (C.c_float * 3)(*hit_last)
+        m = None if means is None else (C.c_double * 6)(*means)
+        acc = ValidationPartial()
+        _check(lib.p2z_validate_partial_device(self.h, _ptr(d_trk_out), bsize, nevts, ntrks, h, m, C.byref(acc),
+                                               stream), self.h)
+        return acc
 
     def relayout_device(self, cfg_from: Config, cfg_to: Config, d_trk_in, d_hits_in, d_trk_out, d_hits_out,
                         d_mask_in=None, d_mask_out=None, stream=None):

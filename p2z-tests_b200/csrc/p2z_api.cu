@@ -57,6 +57,7 @@ struct p2z_context {
   unsigned int *d_status = nullptr;         // device status word
   unsigned long long *d_queue = nullptr;    // 2 persistent work counters (one per copy stream)
   DevBuf trk, hits, out, mask, valid;       // p2z_run buffers / internal masks
+  DevBuf aux;                               // scratch of the validation reduction
   bool has_graph = false;
   GraphKey gkey;
   cudaGraphExec_t gexec = nullptr;
@@ -411,6 +412,10 @@ void set_context_free_error(const char *msg) { fail(nullptr, P2Z_OK, "%s", msg);
 int context_device(const p2z_context *ctx) { return ctx->device; }
 cudaStream_t context_stream(const p2z_context *ctx) { return ctx->stream; }
 p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg) { return fail(ctx, st, "%s", msg); }
+// Device scratch owned by the context, at least `bytes` long (nullptr on failure).
+void *context_scratch(p2z_context *ctx, size_t bytes) {
+  return ensure(ctx, ctx->aux, bytes) == P2Z_OK ? ctx->aux.p : nullptr;
+}
 p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule) {
   Plan pl;
   p2z_status r = make_plan(ctx, cfg, pl);
@@ -514,7 +519,7 @@ p2z_status p2z_destroy(p2z_context *c) {
   for (int i = 0; i < 2; ++i)
     if (c->copy[i]) cudaStreamSynchronize(c->copy[i]);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
-  for (DevBuf *b : {&c->trk, &c->hits, &c->out, &c->mask, &c->valid})
+  for (DevBuf *b : {&c->trk, &c->hits, &c->out, &c->mask, &c->valid, &c->aux})
     if (b->p) cudaFree(b->p);
   if (c->d_status) cudaFree(c->d_status);
   if (c->d_queue) cudaFree(c->d_queue);

@@ -9,10 +9,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
 #include "p2z.h"
+#include "p2z_gen.h"
 
 namespace {
 
@@ -74,48 +76,6 @@ class RefGauss {
 // builds compile with FMA contraction on (gcc -O3 -march=native), which turns
 // this expression into one fused multiply-add; that rounding is kept here.
 inline double smear_factor(double smear, float r) { return std::fma(smear, (double)r, 1.0); }
-
-// ---------------------------------------------------------------------------
-// Counter-based generator for the physics workload
-// ---------------------------------------------------------------------------
-// SplitMix64 (Steele, Lea, Flood 2014) finaliser applied to a per-track key
-// and a counter: the i-th draw of track t depends only on (seed, t, i).
-inline uint64_t mix64(uint64_t z) {
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
-struct TrackRng {
-  uint64_t key, ctr = 0;
-  TrackRng(uint64_t seed, uint64_t stream) : key(mix64(seed + 0x9E3779B97F4A7C15ull * (stream + 1))) {}
-  uint64_t bits() { return mix64(key + 0x9E3779B97F4A7C15ull * (++ctr)); }
-  double uniform() { return ((double)(bits() >> 11) + 0.5) * (1.0 / 9007199254740992.0); }  // (0,1)
-  double normal() {  // Box-Muller, one variate per call
-    const double u1 = uniform(), u2 = uniform();
-    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
-  }
-};
-
-// Cholesky of a symmetric 6x6 (row-major); false if not positive definite.
-bool cholesky6(const double A[6][6], double L[6][6]) {
-  for (int i = 0; i < 6; ++i)
-    for (int j = 0; j < 6; ++j) L[i][j] = 0.0;
-  for (int j = 0; j < 6; ++j) {
-    double d = A[j][j];
-    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-    if (!(d > 1e-12)) return false;
-    L[j][j] = std::sqrt(d);
-    for (int i = j + 1; i < 6; ++i) {
-      double s = A[i][j];
-      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-      L[i][j] = s / L[j][j];
-    }
-  }
-  return true;
-}
-
-inline int sym(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
 int host_threads(int requested) {
   if (requested > 0) return requested;
@@ -233,84 +193,19 @@ p2z_status p2z_generate_physics(const p2z_physics_params *p, const p2z_config *c
   const uint32_t all = nlayer >= 32 ? 0xffffffffu : ((1u << nlayer) - 1u);
   float *T = (float *)trk_out;
   float *H = (float *)hits_out;
-  const double lpt0 = std::log(p->pt_min), lpt1 = std::log(p->pt_max);
   parallel_for(nslots, host_threads(p->nthreads), [&](int64_t s0, int64_t s1) {
     for (int64_t s = s0; s < s1; ++s) {
       const int64_t b = s / B;
       const int t = (int)(s % B);
-      float *tb = T + b * (int64_t)TRK_WORDS * B;
+      const p2z_gen::SlotView view{T + b * (int64_t)TRK_WORDS * B, H + b * nlayer * (int64_t)HIT_WORDS * B, t, B};
       const int64_t e = batch_event[b];
       const bool real = (s - ev_first[e]) < ev_n[e];
       if (!real) {
-        for (int w = 0; w < TRK_WORDS; ++w) tb[t + w * B] = 0.f;
-        for (int l = 0; l < nlayer; ++l) {
-          float *hb = H + (b * nlayer + l) * (int64_t)HIT_WORDS * B;
-          for (int w = 0; w < HIT_WORDS; ++w) hb[t + w * B] = 0.f;
-        }
+        p2z_gen::zero_slot(nlayer, view);
         if (hit_mask) hit_mask[s] = 0u;
         continue;
       }
-      TrackRng r(p->seed, (uint64_t)s);
-      const int q = r.uniform() < 0.5 ? -1 : 1;
-      const double pt = std::exp(lpt0 + (lpt1 - lpt0) * r.uniform());
-      const double ipt = 1.0 / pt;
-      const double phi = -M_PI + 2.0 * M_PI * r.uniform();
-      const double eta = p->eta_min + (p->eta_max - p->eta_min) * r.uniform();
-      const double theta = 2.0 * std::atan(std::exp(-eta));
-      const double vz = p->sigma_vz * r.normal();
-      const double truth[6] = {0.0, 0.0, vz, ipt, phi, theta};
-      const double sig[6] = {p->sig_xy, p->sig_xy, p->sig_z, p->rel_sig_ipt * ipt, p->sig_phi, p->sig_theta};
-      // random correlation, |rho| <= rho_max, positive definite
-      double rho[6][6], L[6][6];
-      bool ok = false;
-      for (int attempt = 0; attempt < 64 && !ok; ++attempt) {
-        const double shrink = attempt < 32 ? 1.0 : std::pow(0.5, attempt - 31);
-        for (int i = 0; i < 6; ++i) {
-          rho[i][i] = 1.0;
-          for (int j = 0; j < i; ++j) rho[i][j] = rho[j][i] = shrink * p->rho_max * (2.0 * r.uniform() - 1.0);
-        }
-        ok = cholesky6(rho, L);
-      }
-      if (!ok) {
-        for (int i = 0; i < 6; ++i)
-          for (int j = 0; j < 6; ++j) rho[i][j] = i == j ? 1.0 : 0.0;
-        cholesky6(rho, L);
-      }
-      // initial state = truth + D L n
-      double n6[6];
-      for (int i = 0; i < 6; ++i) n6[i] = r.normal();
-      double par[6];
-      for (int i = 0; i < 6; ++i) {
-        double acc = 0.0;
-        for (int k = 0; k <= i; ++k) acc += L[i][k] * n6[k];
-        par[i] = truth[i] + sig[i] * acc;
-      }
-      for (int i = 0; i < 6; ++i) tb[t + i * B] = (float)par[i];
-      for (int i = 0; i < 6; ++i)
-        for (int j = 0; j <= i; ++j) tb[t + (6 + sym(i, j)) * B] = (float)(sig[i] * rho[i][j] * sig[j]);
-      std::memcpy(&tb[t + 27 * B], &q, sizeof q);
-      // hits on the planes, at the true helix point plus noise
-      const double k = q * kf;
-      const double cP = std::cos(phi), sP = std::sin(phi);
-      const double tanT = std::tan(theta);
-      for (int l = 0; l < nlayer; ++l) {
-        const double zl = nlayer > 1 ? p->z_first + (p->z_last - p->z_first) * l / (nlayer - 1) : p->z_first;
-        const double alpha = (zl - vz) * tanT * ipt / k;
-        const double sa = std::sin(alpha), ca = std::cos(alpha);
-        const double hx = truth[0] + k * pt * (cP * sa - sP * (1.0 - ca));
-        const double hy = truth[1] + k * pt * (sP * sa + cP * (1.0 - ca));
-        float *hb = H + (b * nlayer + l) * (int64_t)HIT_WORDS * B;
-        hb[t + 0 * B] = (float)(hx + p->hit_sig_xy * r.normal());
-        hb[t + 1 * B] = (float)(hy + p->hit_sig_xy * r.normal());
-        hb[t + 2 * B] = (float)(zl + p->hit_sig_z * r.normal());
-        const float vxy = (float)(p->hit_sig_xy * p->hit_sig_xy), vz2 = (float)(p->hit_sig_z * p->hit_sig_z);
-        hb[t + 3 * B] = vxy;
-        hb[t + 4 * B] = 0.f;
-        hb[t + 5 * B] = vxy;
-        hb[t + 6 * B] = 0.f;
-        hb[t + 7 * B] = 0.f;
-        hb[t + 8 * B] = vz2;
-      }
+      p2z_gen::generate_slot(*p, kf, nlayer, (uint64_t)s, view);
       if (hit_mask) hit_mask[s] = all;
     }
   });
@@ -326,17 +221,7 @@ p2z_status p2z_mask_layers(uint32_t *hit_mask, int64_t nslots, int nlayer, int m
   parallel_for(nslots, host_threads(0), [&](int64_t s0, int64_t s1) {
     for (int64_t s = s0; s < s1; ++s) {
       if (hit_mask[s] == 0u) continue;
-      TrackRng r(seed ^ 0x5bd1e995ull, (uint64_t)s);
-      const int L = min_hits + (int)std::min<double>(max_hits - min_hits, std::floor(r.uniform() * (max_hits - min_hits + 1)));
-      uint32_t m = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
-      int count = L;
-      for (int l = 0; l < L; ++l) {
-        if (count > min_hits && r.uniform() < drop_prob) {
-          m &= ~(1u << l);
-          --count;
-        }
-      }
-      hit_mask[s] = m;
+      hit_mask[s] = p2z_gen::mask_slot(seed, (uint64_t)s, min_hits, max_hits, drop_prob);
     }
   });
   return P2Z_OK;
@@ -451,6 +336,52 @@ void p2z_print_validation(const p2z_validation *v) {
   std::printf("number of tracks with nans=%i\n", (int)v->nnans);
   std::printf("number of tracks failed=%i\n", (int)v->nfail);
   std::fflush(stdout);
+}
+
+p2z_status p2z_dump_tracks(const void *trk_in, const void *trk_out, int bsize, int64_t nevts, int64_t ntrks,
+                           const float hit_last[3], const char *dir) {
+  if (!trk_in || !trk_out || !hit_last) return P2Z_BAD_ARG;
+  if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize) return P2Z_BAD_ARG;
+  const std::string base = (dir && *dir) ? std::string(dir) + "/" : std::string();
+  static const char *names[6] = {"output_x.txt", "output_y.txt", "output_z.txt",
+                                 "input_x.txt",  "input_y.txt",  "input_z.txt"};
+  FILE *f[6] = {};
+  for (int i = 0; i < 6; ++i) {
+    f[i] = std::fopen((base + names[i]).c_str(), "w");
+    if (!f[i]) {
+      for (int j = 0; j < i; ++j) std::fclose(f[j]);
+      return P2Z_BAD_ARG;
+    }
+  }
+  const float *O = (const float *)trk_out, *I = (const float *)trk_in;
+  const int64_t nb = ntrks / bsize;
+  const double hx_ = hit_last[0], hy_ = hit_last[1], hz_ = hit_last[2];
+  // the validation's selection (src/propagate-toz-test_OMP.cpp:758-795); the
+  // dump's lines (src/propagate-toz-test_CUDA_v4.cu:1051-1055, :1129-1136)
+  for (int64_t ie = 0; ie < nevts; ++ie)
+    for (int64_t it = 0; it < ntrks; ++it) {
+      const int64_t off = ((it / bsize) + nb * ie) * (int64_t)TRK_WORDS * bsize + (it % bsize);
+      const float *b = O + off;
+      const double x_ = b[0], y_ = b[bsize], z_ = b[2 * bsize];
+      const double pt_ = 1. / b[3 * bsize], phi_ = b[4 * bsize], theta_ = b[5 * bsize];
+      if (!(std::isfinite(x_) && std::isfinite(y_) && std::isfinite(z_) && std::isfinite(pt_) &&
+            std::isfinite(phi_) && std::isfinite(theta_)))
+        continue;
+      if (std::fabs((x_ - hx_) / hx_) > 1. || std::fabs((y_ - hy_) / hy_) > 1. || std::fabs((z_ - hz_) / hz_) > 1. ||
+          std::fabs((pt_ - 12.) / 12.) > 1. || std::fabs((phi_ - 1.3) / 1.3) > 1. ||
+          std::fabs((theta_ - 2.8) / 2.8) > 1.)
+        continue;
+      const float *a = I + off;
+      std::fprintf(f[0], "%f\n", x_);
+      std::fprintf(f[1], "%f\n", y_);
+      std::fprintf(f[2], "%f\n", z_);
+      std::fprintf(f[3], "%f\n", (double)a[0]);
+      std::fprintf(f[4], "%f\n", (double)a[bsize]);
+      std::fprintf(f[5], "%f\n", (double)a[2 * bsize]);
+    }
+  for (int i = 0; i < 6; ++i) std::fclose(f[i]);
+  return P2Z_OK;
 }
 
 void p2z_print_formatted(int niter, int64_t nevts, int64_t ntrks, int bsize, double wall_s, double setup_s,

@@ -6,15 +6,25 @@ Workload: the single-seed endcap track and hit of the pseudocode
 20 layers.  Conditioning is swept by scaling the track's q/pT uncertainty
 (sigma(q/pT)/|q/pT| from 1e-1 to 1e-6, its covariance row and column rescaled
 so that correlations are kept) and the hit's transverse uncertainty (sigma
-from 1 cm to 1 um, the xy block of V rescaled).  For each point the condition
-number of the first residual covariance R = C + V (xy block) is reported.
+from 1 cm to 1 um, the xy block of V rescaled, its x-y correlation of -0.9988
+kept).  The hit's x-z and y-z covariances are set to zero: with the seed's own
+values (correlations of about 0.03 against sigma_z = 3.4 cm) the 3x3 hit
+covariance is near-singular once its xy block is rescaled (condition number
+1.2e7 at 1 cm to 1.2e13 at 10 um), which only the 3-D update reads and which
+makes that problem ill-posed in any precision; the 2-D updates never read
+them.  For each point the table gives, at the first update of track 0, the
+condition number of R = C + V (xy block, C propagated) and the ratio of the
+track's to the hit's xy sigma, which sets how much the update shrinks C and so
+how much cancellation C - K H C suffers.
 
 References:
-  * 2-D variants: the GPU FP64 kernel on all tracks (pinned to the FP64 host
-    oracle by tests/test_gpu_parity.py::test_other_2d_variants_vs_fp64[f64])
-    and the FP64 host oracle itself on the first `--oracle-tracks` tracks;
+  * 2-D variants: the GPU FP64 kernel on all tracks (itself pinned to the FP64
+    host oracle, agreement printed per point);
   * 3-D (3x3 + Joseph) variants: the FP64 host oracle's 3x3 Joseph update on
-    the first `--oracle-tracks` tracks.
+    the first `--oracle-tracks` tracks;
+  * "float-state floor": the FP64 host oracle run one layer at a time with the
+    track state rounded to FP32 between layers -- the error any variant that
+    stores its state in FP32 (every variant but full FP64) starts from.
 Metrics as in the tests: parameters |d|/max(|ref|, floor), covariance
 |dC_ij|/sqrt(C_ii C_jj).
 
@@ -41,6 +51,7 @@ SIG_HIT_CM = [1.0, 1e-1, 1e-2, 1e-3, 1e-4]
 VARIANTS = [("reference FP32", "v2", 0x20), ("precise FP32", "v2", 0), ("FP64-free compensated", "v2_comp", 0),
             ("3x3 FP64 island + Joseph", "3x3_f64", 0), ("3x3 compensated FP32", "3x3_comp", 0),
             ("full FP64", "f64", 0)]
+COLUMNS = [v[0] for v in VARIANTS] + ["float-state floor (2d)", "float-state floor (3x3)"]
 
 
 def base_workload(p2z, ntracks):
@@ -70,7 +81,7 @@ def conditioned(trk, hit, par, cov, hcov, sig_ipt, sig_hit):
     t[:, 6 + IPT_DIAG, :] *= np.float32(f * f)
     h = hit.copy()
     h[:, :, 3:6, :] *= np.float32(g)
-    h[:, :, 6:8, :] *= np.float32(np.sqrt(g))
+    h[:, :, 6:8, :] = 0.0  # x-z and y-z hit covariances (see the module text)
     # the first update's inputs, for track 0: propagated C (xy block) and V
     b = np.ascontiguousarray(t[0])
     O.step_f32(b, np.ascontiguousarray(h[0, 0]), 0)
@@ -104,6 +115,16 @@ def errors_gpu(torch, out, ref_par, ref_cov):
     q99 = lambda x: float(x.flatten().sort().values[max(0, int(0.99 * x.numel()) - 1)])
     return {"par_max": pr.max(0).values.cpu().numpy(), "cov_max": float(cr.max()), "cov_p99": q99(cr),
             "nonfinite": int((~torch.isfinite(par).all(1)).sum())}
+
+
+def float_state_floor(p2z, trk, hit, update):
+    """FP64 oracle, one layer at a time, state rounded to FP32 in between."""
+    nb, w, B = trk.shape
+    cur = trk.copy()
+    for l in range(hit.shape[1]):
+        o = O.run_f64(cur, np.ascontiguousarray(hit[:, l:l + 1]), update=update)
+        cur[:, :27, :] = o.reshape(nb, B, 27).astype(np.float32).transpose(0, 2, 1)
+    return cur
 
 
 def errors_host(p2z, out, ref64):
@@ -144,6 +165,11 @@ def main():
             o2 = O.run_f64(to, ho)
             o3 = O.run_f64(to, ho, update=O.UPDATE_3X3_JOSEPH)
             f64_vs_oracle = errors_host(p2z, f64_host, o2)
+            floors = {"2d": errors_host(p2z, float_state_floor(p2z, to, ho, O.UPDATE_V2), o2),
+                      "3x3": errors_host(p2z, float_state_floor(p2z, to, ho, O.UPDATE_3X3_JOSEPH), o3)}
+            for kind, e in floors.items():
+                rows.append({"sig_ipt": si, "sig_hit_cm": sh, "cond": cond, "shrink": shrink,
+                             "variant": f"float-state floor ({kind})", **e, "f64_vs_oracle_par_max": 0.0})
             for name, upd, fl in VARIANTS:
                 out = torch.empty_like(dt)
                 ctx.run_device(cfg(upd, fl), dt, dh, out)
@@ -161,20 +187,21 @@ def main():
     names = ["x", "y", "z", "ipt", "phi", "theta"]
     lines = ["# Precision study: every update variant against FP64 across a conditioning sweep", "",
              "Generated by `python tests/precision_study.py --tracks %d --out <this file>` on one B200." % args.tracks,
-             "", __doc__.split("\n\n")[1], "",
+             "", __doc__.split("\n\n")[1], "", __doc__.split("\n\n")[2], "",
              "Rows: sigma(q/pT) relative; hit sigma (cm); at the first update of track 0, the condition number of R = C + V "
              "(xy block, C propagated) and the ratio sigma_track/sigma_hit in xy (how far the update shrinks C).",
              f"2-D variants against the GPU FP64 kernel on all {ntr} tracks; 3x3 variants against the "
-             f"FP64 host oracle's 3x3 Joseph update on the first {nb_o * B} tracks.",
+             f"FP64 host oracle's 3x3 Joseph update on the first {nb_o * B} tracks; float-state floors on "
+             f"those {nb_o * B} tracks.",
              "Cells: max relative error of the worst parameter / max normalised covariance error "
              "(non-finite tracks in brackets when any).", ""]
-    hdr = "| sigma(q/pT) | hit sigma | cond(R) | track/hit sigma | " + " | ".join(v[0] for v in VARIANTS) + " |"
-    lines += [hdr, "|" + "---|" * (4 + len(VARIANTS))]
+    hdr = "| sigma(q/pT) | hit sigma | cond(R) | track/hit sigma | " + " | ".join(COLUMNS) + " |"
+    lines += [hdr, "|" + "---|" * (4 + len(COLUMNS))]
     for si in SIG_IPT:
         for sh in SIG_HIT_CM:
             rs = [r for r in rows if r["sig_ipt"] == si and r["sig_hit_cm"] == sh]
             cells = []
-            for name, _, _ in VARIANTS:
+            for name in COLUMNS:
                 r = next(x for x in rs if x["variant"] == name)
                 c = f"{r['par_max'].max():.1e} / {r['cov_max']:.1e}"
                 if r["nonfinite"]:
@@ -187,7 +214,7 @@ def main():
     for r in rows:
         lines.append(f"| {r['sig_ipt']:g} | {r['sig_hit_cm']:g} | {r['variant']} | " +
                      " | ".join(f"{v:.1e}" for v in r["par_max"]) + f" | {r['cov_p99']:.1e} |")
-    lines += ["", "GPU FP64 kernel vs FP64 host oracle (worst parameter, per point): " +
+    lines += ["", "GPU FP64 kernel vs FP64 host oracle, 2-D update (worst parameter, per point): " +
               ", ".join(f"{r['f64_vs_oracle_par_max']:.1e}" for r in rows if r["variant"] == "full FP64")]
     text = "\n".join(lines) + "\n"
     if args.out:

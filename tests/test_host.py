@@ -173,3 +173,27 @@ def test_driver_prints_reference_lines_without_gpu(p2z):
                        capture_output=True, text=True, timeout=120)
     assert "track in pos: x=20.048365" in r.stdout
     assert "hit in layer=19, pos: x=7.320264, y=27.722622, z=-80.523956" in r.stdout
+
+
+def test_dump_tracks_writes_the_selected_tracks(p2z, tmp_path):
+    """DUMP_OUTPUT files: one "%f" line per track passing the validation's
+    NaN test and window, output coordinates and input coordinates."""
+    trk_in = p2z.empty_tracks(1, 8)
+    trk_in[0, :3, :] = np.arange(24, dtype=np.float32).reshape(3, 8)
+    out = p2z.empty_tracks(1, 8)
+    out[0, 0, :] = 18.5
+    out[0, 1, :] = 79.8
+    out[0, 2, :] = -80.5
+    out[0, 3, :] = 1 / 12.0
+    out[0, 4, :] = 1.3
+    out[0, 5, :] = 2.8
+    out[0, 0, 2] = np.nan      # dropped: not finite
+    out[0, 5, 5] = 9.0         # dropped: theta outside the window
+    out[0, 0, 7] = 18.25
+    p2z.dump_tracks(trk_in, out, 8, 1, 8, [18.5, 79.8, -80.5], tmp_path)
+    kept = [0, 1, 3, 4, 6, 7]
+    ox = (tmp_path / "output_x.txt").read_text().split()
+    assert ox == ["%f" % v for v in out[0, 0, kept].astype(np.float64)]
+    for name, row in (("input_x.txt", 0), ("input_y.txt", 1), ("input_z.txt", 2)):
+        assert (tmp_path / name).read_text().split() == ["%f" % v for v in trk_in[0, row, kept].astype(np.float64)]
+    assert len((tmp_path / "output_z.txt").read_text().split()) == len(kept)
