@@ -43,14 +43,21 @@ def test_device_block_after_a_pass(p2z, ctx, bsize):
     do = torch.empty_like(dt)
     ctx.run_device(cfg, dt, dh, do)
     out = do.cpu().numpy()
-    # a window point inside the physics sample, so that the block has good tracks
-    hit_last = [float(np.median(out[:, 0, :])), float(np.median(out[:, 1, :])), float(np.median(out[:, 2, :]))]
+    # move the angles into the reference's fixed window (phi ~ 1.3, theta ~ 2.8;
+    # the physics sample is forward, theta ~ 0.2-0.4) and pick a window point
+    # inside the sample, so that the block has good and failed tracks alike
+    out[:, 0, :] += 50.0
+    out[:, 1, :] += 50.0
+    out[:, 4, :] = 1.3 + 0.5 * np.sin(out[:, 4, :])
+    out[:, 5, :] = 2.5 + out[:, 5, :]
+    out[:, 4, ::7] = 10.0  # outside the window: failed tracks
+    hit_last = [50.0, 50.0, float(np.median(out[:, 2, :]))]
     out[0, 0, 3] = np.nan
     do.copy_(torch.from_numpy(out))
     v_host = p2z.validate(out, bsize, 6, 4800, hit_last)
     v_dev = ctx.validate_device(do, bsize, 6, 4800, hit_last)
     _compare(p2z, v_dev, v_host)
-    assert v_dev.nnans == 1
+    assert v_dev.nnans == 1 and v_dev.ngood > 1000 and v_dev.nfail > 1000
     # the per-shard form: pass 1 then pass 2 on the global means
     p1 = ctx.validate_partial_device(do, bsize, 6, 4800, hit_last)
     means = np.array(p1.sum[:6]) / p1.ngood
