@@ -63,7 +63,7 @@ typedef enum p2z_status {
   P2Z_OOM = 2,               /* device or pinned-host allocation failed / budget exceeded */
   P2Z_NONFINITE_INPUT = 3,   /* P2Z_FLAG_CHECK_INPUTS found a NaN/Inf in the inputs */
   P2Z_SINGULAR = 4,          /* P2Z_FLAG_STRICT: a residual covariance had det <= 0 */
-  P2Z_TIMEOUT = 5,           /* a bounded wait ran out */
+  P2Z_TIMEOUT = 5,           /* a bounded wait ran out (serving, or a staged kernel's copy wait) */
   P2Z_CUDA_ERROR = 6,        /* a CUDA runtime call failed; see p2z_last_error() */
   P2Z_NO_DEVICE = 7,         /* no usable CUDA device */
   P2Z_UNSUPPORTED = 8,       /* valid but not built (e.g. an unsupported bsize) */
@@ -93,12 +93,18 @@ typedef enum p2z_update_kind {
  *  PER_EVENT   one launch per event (the reference's launch-per-chunk form,
  *              src/propagate-toz-test_CUDA_v4.cu:970-986, taken down to one event per launch).
  *  PERSISTENT  one persistent launch (grid = resident CTAs) whose warps take
- *              32-slot work items from a device queue; replayed as a CUDA graph. */
+ *              32-slot work items from a device queue; replayed as a CUDA graph.
+ *  STAGED      the persistent form with each warp's hit tiles streamed through
+ *              shared memory by bulk asynchronous copies, several layers ahead,
+ *              and the next batch's tracks copied in during the current one.
+ *              bsize 32, AOSOA layout and 16-byte aligned track and hit arrays
+ *              only (P2Z_UNSUPPORTED otherwise).  p2z_run runs its chunks flat. */
 typedef enum p2z_schedule {
   P2Z_SCHED_AUTO = 0,
   P2Z_SCHED_FLAT = 1,
   P2Z_SCHED_PER_EVENT = 2,
-  P2Z_SCHED_PERSISTENT = 3
+  P2Z_SCHED_PERSISTENT = 3,
+  P2Z_SCHED_STAGED = 4
 } p2z_schedule;
 
 /* Array layouts (see the top of this file). */
@@ -261,7 +267,7 @@ p2z_status p2z_relayout_device(p2z_context *ctx, const p2z_config *from, const p
 typedef struct p2z_tune_entry {
   int32_t bsize;          /* 8, 16, 32, 64 */
   int32_t layout;         /* p2z_layout */
-  int32_t schedule;       /* P2Z_SCHED_FLAT, _PER_EVENT or _PERSISTENT */
+  int32_t schedule;       /* P2Z_SCHED_FLAT, _PER_EVENT, _PERSISTENT or _STAGED */
   int32_t block_threads;  /* 32 .. 256 */
   double ms;              /* mean device time of one pass */
   double updates_per_s;   /* present-hit updates per second */
@@ -269,8 +275,9 @@ typedef struct p2z_tune_entry {
 
 /* Autotuner: measures one pass of cfg's work (its update kind and flags, one
  * iteration) on the caller's device data under every combination of bsize
- * {8,16,32,64} x layout {AOSOA, SOA} x schedule {FLAT, PERSISTENT, and
- * PER_EVENT when nevts <= 4096} x block_threads {32,64,128,256}, each the mean
+ * {8,16,32,64} x layout {AOSOA, SOA} x schedule {FLAT, PERSISTENT, PER_EVENT
+ * when nevts <= 4096, and STAGED at bsize 32 AOSOA} x block_threads
+ * {32,64,128,256}, each the mean
  * of `reps` passes (0 -> 3) after one warm-up pass.  The inputs are converted
  * to each candidate's bsize and layout with p2z_relayout_device into scratch
  * buffers the call allocates and frees (about twice the input size); the

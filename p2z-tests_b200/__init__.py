@@ -37,9 +37,9 @@ UPDATE_V2, UPDATE_V2_COMP, UPDATE_3X3_F64, UPDATE_3X3_COMP, UPDATE_F64 = range(5
 UPDATE_NAMES = {"v2": UPDATE_V2, "v2_comp": UPDATE_V2_COMP, "3x3_f64": UPDATE_3X3_F64,
                 "3x3_comp": UPDATE_3X3_COMP, "f64": UPDATE_F64}
 # schedules
-SCHED_AUTO, SCHED_FLAT, SCHED_PER_EVENT, SCHED_PERSISTENT = range(4)
+SCHED_AUTO, SCHED_FLAT, SCHED_PER_EVENT, SCHED_PERSISTENT, SCHED_STAGED = range(5)
 SCHED_NAMES = {"auto": SCHED_AUTO, "flat": SCHED_FLAT, "per_event": SCHED_PER_EVENT,
-               "persistent": SCHED_PERSISTENT}
+               "persistent": SCHED_PERSISTENT, "staged": SCHED_STAGED}
 SCHED_LABELS = {v: k for k, v in SCHED_NAMES.items()}
 # array layouts
 LAYOUT_AOSOA, LAYOUT_SOA = 0, 1

@@ -33,7 +33,7 @@ struct DevBuf {
 
 struct GraphKey {
   RunArgs args;
-  int bsize, upd, sc, block, grid;
+  int bsize, upd, sc, block, grid, kind;
   bool masked, soa;
   bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -135,7 +135,7 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
   if (cfg->nevts < 0) return fail(ctx, P2Z_BAD_ARG, "nevts %lld < 0", (long long)cfg->nevts);
   if (cfg->update < P2Z_UPDATE_V2 || cfg->update > P2Z_UPDATE_F64)
     return fail(ctx, P2Z_BAD_ARG, "update kind %d unknown", cfg->update);
-  if (cfg->schedule < P2Z_SCHED_AUTO || cfg->schedule > P2Z_SCHED_PERSISTENT)
+  if (cfg->schedule < P2Z_SCHED_AUTO || cfg->schedule > P2Z_SCHED_STAGED)
     return fail(ctx, P2Z_BAD_ARG, "schedule %d unknown", cfg->schedule);
   if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
     return fail(ctx, P2Z_BAD_ARG, "block_threads %d not a multiple of 32 in 32..256", cfg->block_threads);
@@ -263,8 +263,12 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
     ++*launches;
     return P2Z_OK;
   }
-  // persistent
-  spec.kind = KIND_PERSISTENT;
+  // persistent (staged or not)
+  spec.kind = schedule == P2Z_SCHED_STAGED ? KIND_STAGED : KIND_PERSISTENT;
+  if (spec.kind == KIND_STAGED &&
+      (pl.B != 32 || pl.soa || (((uintptr_t)base.trk | (uintptr_t)base.hits) & 15u) != 0 || s0 % 32 || s1 % 32))
+    return fail(ctx, P2Z_UNSUPPORTED, "the staged schedule needs bsize 32, the AOSOA layout and 16-byte aligned "
+                                      "track and hit arrays");
   const int occ = occupancy(spec);
   if (occ <= 0) return fail(ctx, P2Z_CUDA_ERROR, "occupancy query failed for the persistent kernel");
   const int64_t items = (s1 - s0 + 31) / 32;
@@ -289,6 +293,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   key.grid = spec.grid;
   key.masked = spec.masked;
   key.soa = spec.soa;
+  key.kind = spec.kind;
   if (!(ctx->has_graph && ctx->gkey == key)) {
     if (ctx->gexec) {
       cudaGraphExecDestroy(ctx->gexec);
@@ -581,6 +586,7 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
     if (r != P2Z_OK) return r;
     stats->launches = launches;
     stats->singular = (status & 1u) ? 1 : 0;
+    if (status & 2u) return fail(ctx, P2Z_TIMEOUT, "a staged kernel's wait for a bulk copy ran out");
     if ((pl.flags & P2Z_FLAG_STRICT) && stats->singular)
       return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
   } else {
@@ -672,7 +678,8 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
         h2d += nbc * pl.B * 4;
       }
       if (!per_event) {
-        r = enqueue_pass(ctx, pl, base, b0 * pl.B, b1 * pl.B, schedule == P2Z_SCHED_PERSISTENT ? P2Z_SCHED_FLAT : schedule,
+        r = enqueue_pass(ctx, pl, base, b0 * pl.B, b1 * pl.B,
+                         (schedule == P2Z_SCHED_PERSISTENT || schedule == P2Z_SCHED_STAGED) ? P2Z_SCHED_FLAT : schedule,
                          st, ctx->d_queue + (c & 1), &launches);
         if (r != P2Z_OK) return r;
         if (pl.soa) {

@@ -32,7 +32,7 @@ constexpr int TRK_WORDS = 28;  // 6 par + 21 cov + 1 q
 constexpr int HIT_WORDS = 9;   // 3 pos + 6 cov
 
 // Kernel kinds
-enum { KIND_FLAT = 0, KIND_PERSISTENT = 1 };
+enum { KIND_FLAT = 0, KIND_PERSISTENT = 1, KIND_STAGED = 2 };
 // Arithmetic of a kernel instance:
 //  UPDK_V2       precise FP32 form, FP64 x/y/phi accumulators, the reference's 2-D update
 //  UPDK_V2_COMP  precise FP32 form with no FP64 at all: float-pair accumulators,
@@ -70,7 +70,7 @@ struct RunArgs {
   int64_t slot_begin, slot_end;    // slots [begin, end) of this launch
   int nlayer;
   float kfact;
-  unsigned int *status;            // bit 0: a det <= 0 was met
+  unsigned int *status;            // bit 0: a det <= 0 was met; bit 1: a staging wait timed out
   unsigned long long *queue;       // persistent kernels: next work item
   int64_t ws;                      // SoA layout (B == 0): slots in the arrays = word stride
 };
@@ -119,7 +119,7 @@ __device__ __forceinline__ void load_hit(HitRegs<NH> &h, const float *p, int64_t
 // input covariance in b21).  Returns true if the update met det <= 0.
 template <int UPD, int SC, bool GENERAL>
 __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<UPD>::A> &s,
-                                     const typename Types<UPD>::T (&b21)[21], const HitRegs<Types<UPD>::NH> &h,
+                                     const typename Types<UPD>::T *b21, const HitRegs<Types<UPD>::NH> &h,
                                      typename Types<UPD>::T k, typename Types<UPD>::T ik) {
   using T = typename Types<UPD>::T;
   const T zout = T(h.w[2]);
@@ -310,6 +310,291 @@ __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArg
   }
 }
 
+// ---------------------------------------------------------------------------
+// Staged persistent kernel (bsize 32, AOSOA): each warp owns one 32-track
+// batch at a time.  Its hit tiles -- the NH contiguous words x 32 lanes of a
+// hit batch, 768 B for the 2-D updates -- stream through a ring of
+// kStages shared-memory buffers filled by bulk asynchronous copies
+// (cp.async.bulk, completion counted on an mbarrier per buffer), issued by
+// lane 0 up to kStages layers ahead and across into the warp's next batch; the
+// next batch's 3584-B track tile is copied in while the current batch runs.
+// Registers hold no prefetched hits and no load of the hot loop waits on DRAM.
+// Hit masks: the warp stages the union of its lanes' layers in order; a lane
+// steps only on its own layers.  Every wait is bounded: on a timeout the warp
+// sets status bit 1, waits (bounded) for the copies it issued and returns.
+// ---------------------------------------------------------------------------
+constexpr int kStages = 4;
+constexpr int kStagedWaitLimit = 1 << 21;  // try_wait polls per wait
+
+template <int UPD>
+struct StagedSmem {
+  static constexpr uint32_t kTrkBytes = TRK_WORDS * 32 * 4;          // 3584
+  static constexpr uint32_t kHitBytes = Types<UPD>::NH * 32 * 4;     // 768 or 1152
+  static constexpr uint32_t kBarOff = kTrkBytes + kStages * kHitBytes;
+  static constexpr uint32_t kWarpBytes = (kBarOff + (kStages + 1) * 8 + 127) / 128 * 128;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < kStagedWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// The same for a whole warp, polled in lockstep so that the warp leaves the
+// loop converged; true when every lane saw the phase complete.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < kStagedWaitLimit; ++i)
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+  return false;
+}
+// Global -> this CTA's shared memory, bytes a multiple of 16, both addresses
+// 16-byte aligned; completion adds the bytes to the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int UPD, int SC, bool MASKED>
+__global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_staged(RunArgs a) {
+  constexpr int B = 32;
+  constexpr int NH = Types<UPD>::NH;
+  using SM = StagedSmem<UPD>;
+  using T = typename Types<UPD>::T;
+  using A = typename Types<UPD>::A;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *wb = smem + (size_t)warp * SM::kWarpBytes;
+  float *trk_s = reinterpret_cast<float *>(wb);
+  float *hit_s = reinterpret_cast<float *>(wb + SM::kTrkBytes);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(wb + SM::kBarOff);  // [0, kStages): hits; [kStages]: track
+  if (lane == 0) {
+    for (int i = 0; i <= kStages; ++i) mbar_init(&bars[i], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+
+  const int nl = a.nlayer;
+  const uint32_t all = (nl >= 32) ? 0xffffffffu : ((1u << nl) - 1u);
+  const int S = nl < kStages ? nl : kStages;  // buffers in use
+  const int64_t b0 = a.slot_begin / B;
+  const unsigned long long nitems = (unsigned long long)((a.slot_end - a.slot_begin) / B);
+  auto grab = [&]() -> unsigned long long {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(a.queue, 1ull);
+    return __shfl_sync(0xffffffffu, it, 0);
+  };
+  // lane's mask and the warp's union of layers for an item
+  auto lane_mask = [&](unsigned long long it) -> uint32_t {
+    if (it >= nitems) return 0u;
+    return MASKED ? (__ldg(a.mask + (b0 + (int64_t)it) * B + lane) & all) : all;
+  };
+  auto hit_src = [&](unsigned long long it, int l) -> const float * {
+    return a.hits + ((b0 + (int64_t)it) * nl + l) * (int64_t)(HIT_WORDS * B);
+  };
+  auto trk_src = [&](unsigned long long it) -> const float * {
+    return a.trk + (b0 + (int64_t)it) * (int64_t)(TRK_WORDS * B);
+  };
+
+  unsigned long long item = grab();
+  unsigned long long next = (item < nitems) ? grab() : nitems;
+  uint32_t m_cur = lane_mask(item), m_next = lane_mask(next);
+  uint32_t u_cur = __reduce_or_sync(0xffffffffu, m_cur), u_next = __reduce_or_sync(0xffffffffu, m_next);
+  // producer state (warp-uniform): buffer of the next copy, copies in flight
+  // ahead of the consumer, source (item or next) and its layers left
+  int p_st = 0, ahead = 0;
+  int p_sel = 0;
+  uint32_t p_bits = u_cur;
+  // consumer state: buffer of the next tile and its phase parity
+  int c_st = 0;
+  uint32_t c_par = 0;
+  uint32_t tpar = 0;    // track barrier parity
+  bool trk_pending = false;
+  // issue hit copies while fewer than S are ahead of the consumer; the
+  // bookkeeping is warp-uniform (every lane runs it), lane 0 issues
+  auto produce = [&]() {
+    while (ahead < S) {
+      if (p_bits == 0u && p_sel == 0) {
+        p_sel = 1;
+        p_bits = u_next;
+      }
+      if (p_bits == 0u) break;
+      const int l = __ffs(p_bits) - 1;
+      p_bits &= p_bits - 1u;
+      if (lane == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bars[p_st], SM::kHitBytes);
+        bulk_g2s(hit_s + p_st * (NH * B), hit_src(p_sel ? next : item, l), SM::kHitBytes, &bars[p_st]);
+      }
+      if (++p_st == S) p_st = 0;
+      ++ahead;
+    }
+    __syncwarp();
+  };
+  if (item < nitems && lane == 0) {
+    mbar_arrive_expect_tx(&bars[kStages], SM::kTrkBytes);
+    bulk_g2s(trk_s, trk_src(item), SM::kTrkBytes, &bars[kStages]);
+  }
+  trk_pending = item < nitems;
+  produce();
+  bool ok = true;
+  while (item < nitems) {
+    // the item's track tile
+    ok = mbar_wait_warp(&bars[kStages], tpar);
+    if (!ok) break;
+    tpar ^= 1u;
+    trk_pending = false;
+    float *tout = a.out + (b0 + (int64_t)item) * (int64_t)(TRK_WORDS * B) + lane;
+    if (m_cur == 0u) {  // no hits (or a padding slot): the track passes through
+#pragma unroll
+      for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, trk_s[e * B + lane]);
+    }
+    const int q = __float_as_int(trk_s[27 * B + lane]);
+    const float kf = float(q) * a.kfact;
+    const T k = T(kf);
+    const T ik = T(1) / k;
+    Trk<T, A> s;
+    acc_set(s.x, trk_s[0 * B + lane]);
+    acc_set(s.y, trk_s[1 * B + lane]);
+    acc_set(s.phi, trk_s[4 * B + lane]);
+    s.z = trk_s[2 * B + lane]; s.ipt = trk_s[3 * B + lane]; s.theta = trk_s[5 * B + lane];
+    if constexpr (UPD != UPDK_F64 && UPD != UPDK_V2_REF) init_direction(s);
+    bool singular = false, first = true;
+    // the track tile stays in use until every lane with hits has run its first
+    // (general) step, which reads the input covariance from it
+    bool tile_busy = true;
+    auto release_tile = [&]() {
+      __syncwarp();
+      if (next < nitems) {
+        if (lane == 0) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(&bars[kStages], SM::kTrkBytes);
+          bulk_g2s(trk_s, trk_src(next), SM::kTrkBytes, &bars[kStages]);
+        }
+        trk_pending = true;
+      }
+      tile_busy = false;
+    };
+    // the next staged hit tile into registers, then refill its buffer
+    auto take_hit = [&](HitRegs<NH> &h) -> bool {
+      if (!mbar_wait_warp(&bars[c_st], c_par)) return false;
+#pragma unroll
+      for (int e = 0; e < NH; ++e) h.w[e] = hit_s[c_st * (NH * B) + e * B + lane];
+      __syncwarp();
+      if (++c_st == S) {
+        c_st = 0;
+        c_par ^= 1u;
+      }
+      --ahead;
+      produce();
+      return true;
+    };
+    auto first_step = [&](const HitRegs<NH> &h) {
+      T b21[21];
+#pragma unroll
+      for (int e = 0; e < 21; ++e) b21[e] = T(trk_s[(6 + e) * B + lane]);
+      singular |= step<UPD, SC, true>(s, b21, h, k, ik);
+      first = false;
+    };
+    if constexpr (!MASKED) {
+      // every lane has every layer: the first is general, the rest reduced
+      HitRegs<NH> h;
+      ok = take_hit(h);
+      if (!ok) break;
+      first_step(h);
+      release_tile();
+      for (int l = 1; l < nl; ++l) {
+        ok = take_hit(h);
+        if (!ok) break;
+        singular |= step<UPD, SC, false>(s, nullptr, h, k, ik);
+      }
+    } else {
+      uint32_t ucur = u_cur;
+      while (ucur) {
+        const int l = __ffs(ucur) - 1;
+        ucur &= ucur - 1u;
+        HitRegs<NH> h;
+        ok = take_hit(h);
+        if (!ok) break;
+        if ((m_cur >> l) & 1u) {
+          if (first) first_step(h);
+          else singular |= step<UPD, SC, false>(s, nullptr, h, k, ik);
+        }
+        if (tile_busy && __all_sync(0xffffffffu, !first || (m_cur >> l) == 0u)) release_tile();
+      }
+    }
+    if (!ok) break;
+    if (tile_busy) release_tile();
+    if (!first) {
+      const float z0 = 0.0f;
+      float o[TRK_WORDS];
+      o[0] = tof(s.x); o[1] = tof(s.y); o[2] = float(s.z);
+      o[3] = float(s.ipt); o[4] = tof(s.phi); o[5] = float(s.theta);
+      float *c = o + 6;
+      c[0] = float(s.c00); c[1] = float(s.c10); c[2] = float(s.c11);
+      c[3] = z0; c[4] = z0; c[5] = z0;
+      c[6] = float(s.c30); c[7] = float(s.c31); c[8] = z0; c[9] = float(s.c33);
+      c[10] = float(s.c40); c[11] = float(s.c41); c[12] = z0; c[13] = float(s.c43); c[14] = float(s.c44);
+      c[15] = float(s.c50); c[16] = float(s.c51); c[17] = z0; c[18] = float(s.c53); c[19] = float(s.c54);
+      c[20] = float(s.c55);
+      o[27] = __int_as_float(q);
+#pragma unroll
+      for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * B, o[e]);
+    }
+    if (singular) atomicOr(a.status, 1u);
+    // advance: the producer's "next" becomes its "item"
+    item = next;
+    m_cur = m_next;
+    u_cur = u_next;
+    next = (item < nitems) ? grab() : nitems;
+    m_next = lane_mask(next);
+    u_next = __reduce_or_sync(0xffffffffu, m_next);
+    if (p_sel == 1) {
+      p_sel = 0;
+    } else {  // the producer had not reached the new item yet
+      p_bits = u_cur;
+    }
+    produce();
+  }
+  if (!ok) {
+    // a wait ran out: report it, then wait (bounded) for the copies this warp issued
+    if (lane == 0) {
+      atomicOr(a.status, 2u);
+      int st = c_st;
+      uint32_t par = c_par;
+      for (int j = 0; j < ahead; ++j) {
+        mbar_wait(&bars[st], par);
+        if (++st == S) {
+          st = 0;
+          par ^= 1u;
+        }
+      }
+      if (trk_pending) mbar_wait(&bars[kStages], tpar);
+    }
+    __syncwarp();
+  }
+}
+
 // Launch description used by the dispatch functions.
 struct LaunchSpec {
   RunArgs args;
@@ -343,7 +628,15 @@ template <int UPD, bool HAS_FAST>
 struct Dispatch {
   template <int B, int SC, bool M>
   static const void *fn(int kind) {
+    if (kind == KIND_STAGED) {
+      if constexpr (B == 32) return (const void *)k_staged<UPD, SC, M>;
+      else return nullptr;
+    }
     return kind == KIND_PERSISTENT ? (const void *)k_persistent<B, UPD, SC, M> : (const void *)k_flat<B, UPD, SC, M>;
+  }
+  // dynamic shared memory of a launch
+  static size_t smem_bytes(const LaunchSpec &s) {
+    return s.kind == KIND_STAGED ? (size_t)(s.block / 32) * StagedSmem<UPD>::kWarpBytes : 0;
   }
   template <int B, int SC>
   static const void *fn_m(bool masked, int kind) {
@@ -372,19 +665,29 @@ struct Dispatch {
     const int64_t n = s.args.slot_end - s.args.slot_begin;
     if (n <= 0) return cudaSuccess;
     int grid;
-    if (s.kind == KIND_PERSISTENT) {
+    if (s.kind == KIND_PERSISTENT || s.kind == KIND_STAGED) {
       grid = s.grid;
     } else {
       grid = (int)((n + s.block - 1) / s.block);
     }
+    const size_t smem = smem_bytes(s);
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
     RunArgs a = s.args;
     void *params[] = {&a};
-    return cudaLaunchKernel(f, dim3(grid), dim3(s.block), params, 0, st);
+    return cudaLaunchKernel(f, dim3(grid), dim3(s.block), params, smem, st);
   }
   static int occupancy(const LaunchSpec &s) {
     const void *f = select(s);
     int nb = 0;
-    if (!f || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, s.block, 0) != cudaSuccess) return 0;
+    const size_t smem = smem_bytes(s);
+    if (!f) return 0;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, s.block, smem) != cudaSuccess) return 0;
     return nb;
   }
 };

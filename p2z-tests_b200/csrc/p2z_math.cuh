@@ -464,7 +464,7 @@ __device__ __forceinline__ void propagate_cov_reduced(Trk<T, A> &s, const Jac<T>
 // a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663), which the Jacobian
 // functions fill for the first layer.
 template <typename T, typename A>
-__device__ __forceinline__ void propagate_cov_general(Trk<T, A> &s, const T (&b)[21], const Helix<T> &h,
+__device__ __forceinline__ void propagate_cov_general(Trk<T, A> &s, const T *b, const Helix<T> &h,
                                                       const Jac<T> &J) {
   (void)h;
   const T a2 = J.a2, a8 = J.a8, a26 = J.a26;

@@ -240,6 +240,8 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
     }
     for (int layout : {(int)P2Z_LAYOUT_AOSOA, (int)P2Z_LAYOUT_SOA}) {
       c.layout = layout;
+      std::vector<int> sch = scheds;
+      if (B == 32 && layout == P2Z_LAYOUT_AOSOA) sch.push_back(P2Z_SCHED_STAGED);
       p2z_status r = relayout(ctx, cfg, &c, d_trk_in, d_hits, d_hit_mask, T, H, (uint32_t *)M, st, scr);
       if (r != P2Z_OK) return r;
       // present-hit updates of one pass
@@ -252,7 +254,7 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
       p2z_tune_entry local;
       std::memset(&local, 0, sizeof local);
       local.ms = -1.0;
-      for (int sched : scheds) {
+      for (int sched : sch) {
         for (int block : kBlock) {
           c.schedule = sched;
           c.block_threads = block;

@@ -361,3 +361,55 @@ def test_full_size_properties(p2z, oracle, ctx):
     o64 = oracle.run_f64(np.ascontiguousarray(trk[idx]), np.ascontiguousarray(hit[idx]))
     gs = p2z.tracks_to_aos(np.ascontiguousarray(out[idx]))
     assert par_rel(gs["par"], o64[:, :6]).max() <= PREC_PAR
+
+
+@pytest.mark.parametrize("update", ["v2", "3x3_f64", "v2_comp", "f64"])
+@pytest.mark.parametrize("masked", [False, True])
+def test_staged_schedule_bitwise_equal(p2z, ctx, update, masked):
+    """The staged kernel (hit tiles streamed through shared memory by bulk
+    copies) runs the same per-track arithmetic as the flat one."""
+    import torch
+    counts = [700, 31, 0, 1500, 64, 2048] if masked else None
+    if counts is None:
+        cfg = p2z.make_config(bsize=32, nevts=3, ntrks=1600, nlayer=20, update=update)
+        t, h = p2z.generate_physics(cfg)
+        m = None
+    else:
+        cfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, update=update)
+        t, h, m = p2z.generate_physics(cfg, with_mask=True)
+        p2z.mask_layers(m, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=29)
+    dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+    dm = None if m is None else torch.from_numpy(m.view(np.int32)).cuda()
+    outs = {}
+    for sched in ("flat", "staged"):
+        cfg.schedule = p2z.SCHED_NAMES[sched]
+        o = torch.full_like(dt, float("nan"))
+        ctx.run_device(cfg, dt, dh, o, d_mask=dm)
+        outs[sched] = o.cpu().numpy()
+    assert _bitdiff(outs["flat"], outs["staged"]) == 0
+
+
+@pytest.mark.parametrize("nlayer", [1, 3, 20])
+def test_staged_schedule_short_tracks(p2z, ctx, nlayer):
+    """Fewer layers than shared-memory buffers, and many small work items."""
+    import torch
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=320, nlayer=nlayer)
+    t, h = p2z.generate_physics(cfg)
+    dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+    outs = []
+    for sched, block in (("flat", 128), ("staged", 32), ("staged", 256)):
+        c = p2z.make_config(bsize=32, nevts=2, ntrks=320, nlayer=nlayer, schedule=sched, block_threads=block)
+        o = torch.full_like(dt, float("nan"))
+        ctx.run_device(c, dt, dh, o)
+        outs.append(o.cpu().numpy())
+    assert _bitdiff(outs[0], outs[1]) == 0 and _bitdiff(outs[0], outs[2]) == 0
+
+
+def test_staged_schedule_rejects_other_layouts(p2z, ctx):
+    import torch
+    cfg = p2z.make_config(bsize=16, nevts=1, ntrks=64, nlayer=4, schedule="staged")
+    t, h = p2z.generate_physics(cfg)
+    dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+    with pytest.raises(p2z.P2zError) as e:
+        ctx.run_device(cfg, dt, dh, torch.empty_like(dt))
+    assert e.value.status == p2z.UNSUPPORTED

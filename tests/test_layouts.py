@@ -205,10 +205,11 @@ def test_autotune_contract(p2z, masked):
         c.run_device(cfg, dt, dh, ref, d_mask=dm, stats=False)
         torch.cuda.synchronize()
         best, rows = c.autotune(cfg, dt, dh, d_mask=dm, reps=2)
-        assert len(rows) == 4 * 2 * 3 * 4
+        assert len(rows) == 4 * 2 * 3 * 4 + 4  # + the staged schedule at bsize 32 AOSOA
         assert {r["bsize"] for r in rows} == {8, 16, 32, 64}
         assert {r["layout"] for r in rows} == {"aosoa", "soa"}
-        assert {r["schedule"] for r in rows} == {"flat", "persistent", "per_event"}
+        assert {r["schedule"] for r in rows} == {"flat", "persistent", "per_event", "staged"}
+        assert {(r["bsize"], r["layout"]) for r in rows if r["schedule"] == "staged"} == {(32, "aosoa")}
         assert {r["block_threads"] for r in rows} == {32, 64, 128, 256}
         assert best["ms"] == min(r["ms"] for r in rows) and best["ms"] > 0
         assert all(r["updates_per_s"] > 0 for r in rows)
