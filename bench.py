@@ -374,6 +374,9 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-events", type=int, default=1500)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "flat", "persistent", "per_event", "staged"],
+                    help="launch schedule of the headline step (auto: what the autotuner measured best)")
+    ap.add_argument("--block", type=int, default=0, help="threads per CTA of the headline step (0: tuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -391,7 +394,8 @@ def main():
 
     nev = args.nevts
     # schedule and block size left open: the context applies what p2z_autotune measured
-    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20)
+    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule=args.schedule,
+                          block_threads=args.block)
     params = p2z.physics_params(seed=20240601 + rank)
     trk, hit = p2z.generate_physics(cfg, params)
     updates = nev * 9600 * 20
@@ -539,8 +543,11 @@ def main():
         "config": {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
                    "updates_per_step_per_gpu": updates, "l2": "inputs 8.1 GB > L2, no flush",
                    "parallelism": f"dp{world} (independent event shards)",
-                   "launch": ({k: tune_head["best_bsize32_aosoa"][k] for k in ("schedule", "block_threads")}
-                              if tune_head else {"schedule": "flat", "block_threads": 128})},
+                   "launch": {"schedule": (args.schedule if args.schedule != "auto" else
+                                           (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
+                              "block_threads": (args.block or
+                                                (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head
+                                                 else 128))}},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": (tpu * updates / launches_per_step) if tpu else None,
