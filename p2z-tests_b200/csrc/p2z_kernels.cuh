@@ -136,6 +136,8 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
     J = jacobian_precise<float, GENERAL>(hx, k, s.ipt);
   }
   if constexpr (GENERAL) propagate_cov_general(s, b21, hx, J);
+  else if constexpr (P2Z_PACKED_F32X2 && std::is_same<T, float>::value && UPD != UPDK_V2_REF)
+    propagate_cov_reduced_packed(s, J);  // (the reference-rounding form keeps separate roundings)
   else propagate_cov_reduced(s, J);
   if constexpr (UPD == UPDK_F64) {
     const double hp[3] = {h.w[0], h.w[1], h.w[2]};

@@ -122,6 +122,16 @@ __device__ __forceinline__ float rcp_nr(float x) {
   return fmaf(r, e, r);
 }
 
+// Packed FP32 pairs: one sm_100 instruction performs two independent FP32
+// operations on a register pair (per component exactly __fmaf_rn / __fmul_rn),
+// halving the issue slots of paired arithmetic.
+#ifndef P2Z_PACKED_F32X2
+#define P2Z_PACKED_F32X2 1
+#endif
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
 // ---------------------------------------------------------------------------
 // sin / cos / versine
 // ---------------------------------------------------------------------------
@@ -459,6 +469,42 @@ __device__ __forceinline__ void propagate_cov_reduced(Trk<T, A> &s, const Jac<T>
   s.c55 = t35;                                           // c20
 }
 
+// The same reduced form with the row-0/row-1 Jacobian pairs (a3, a9),
+// (a4, a10), (a5, a11) and the covariance pairs (c00, c10), (c30, c31),
+// (c40, c41), (c50, c51) in packed FP32 pairs.  Each component is the scalar
+// form's chain of fused multiply-adds in the same order, so the results are
+// identical bit for bit; the pairs only halve the instructions.  Identities
+// used: the new (c30, c31) is T's (t3, t9), the new (c50, c51) is (t5, t11),
+// the new c54 is t29 and the new c43 is t27.
+template <typename A>
+__device__ __forceinline__ void propagate_cov_reduced_packed(Trk<float, A> &s, const Jac<float> &J) {
+  const float2 A3 = make_float2(J.a3, J.a9), A4 = make_float2(J.a4, J.a10), A5 = make_float2(J.a5, J.a11);
+  const float2 P0 = make_float2(s.c00, s.c10), P3 = make_float2(s.c30, s.c31);
+  const float2 P4 = make_float2(s.c40, s.c41), P5 = make_float2(s.c50, s.c51);
+  // T = J C: rows 0 and 1 in pairs (columns 0, 3, 4, 5), row 1 column 1, row 4
+  const float2 T0 = fma2(A5, bc2(s.c50), fma2(A4, bc2(s.c40), fma2(A3, bc2(s.c30), P0)));  // (t0, t6)
+  const float2 T3 = fma2(A5, bc2(s.c53), fma2(A4, bc2(s.c43), fma2(A3, bc2(s.c33), P3)));  // (t3, t9)
+  const float2 T4 = fma2(A5, bc2(s.c54), fma2(A4, bc2(s.c44), fma2(A3, bc2(s.c43), P4)));  // (t4, t10)
+  const float2 T5 = fma2(A5, bc2(s.c55), fma2(A4, bc2(s.c54), fma2(A3, bc2(s.c53), P5)));  // (t5, t11)
+  const float t7 = s.c11 + J.a9 * s.c31 + J.a10 * s.c41 + J.a11 * s.c51;
+  const float2 T24 = fma2(bc2(J.a29), P5, fma2(bc2(J.a27), P3, P4));                        // (t24, t25)
+  const float t27 = J.a27 * s.c33 + s.c43 + J.a29 * s.c53;
+  const float t28 = J.a27 * s.c43 + s.c44 + J.a29 * s.c54;
+  const float t29 = J.a27 * s.c53 + s.c54 + J.a29 * s.c55;
+  // C' = T J^T
+  const float2 N0 = fma2(T5, bc2(J.a5), fma2(T4, bc2(J.a4), fma2(T3, bc2(J.a3), T0)));      // (c00, c10)
+  const float c11 = t7 + T3.y * J.a9 + T4.y * J.a10 + T5.y * J.a11;
+  const float2 N4 = fma2(A5, bc2(t29), fma2(A4, bc2(t28), fma2(A3, bc2(t27), T24)));       // (c40, c41)
+  s.c00 = N0.x; s.c10 = N0.y;
+  s.c11 = c11;
+  s.c30 = T3.x; s.c31 = T3.y;
+  s.c40 = N4.x; s.c41 = N4.y;
+  s.c43 = t27;
+  s.c44 = t27 * J.a27 + t28 + t29 * J.a29;
+  s.c50 = T5.x; s.c51 = T5.y;
+  s.c54 = t29;
+}
+
 // General form on the full 21-element input covariance b[] (the first
 // propagation of a track), including the Jacobian's z column a2 = J(0,2),
 // a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663), which the Jacobian
@@ -520,8 +566,54 @@ __device__ __forceinline__ float det2_comp(float a, float b, float c, float d) {
 // Apply the 2-D (x,y) gain: K(i,:) = (C(i,0), C(i,1)) * Rinv for the live rows
 // (the z row is zero), the parameter update with the residual (hx - x,
 // hy - y), and C - K (H C) (reference :534-617).
+// FORM_PRECISE, FP32 with packed pairs: the gain rows (K_i0, K_i1) as
+// c_i0 (r00, r01) + c_i1 (r01, r11), and C - K (H C) with the column-0/1 pairs
+// of rows y, ipt, phi, theta updated together:
+//   (c_i0, c_i1)' = (c_i0, c_i1) - K_i0 (c00, c10) - K_i1 (c10, c11).
+template <typename A>
+__device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r00, float r01, float r11, float hx,
+                                                       float hy) {
+  const float2 R0 = make_float2(r00, r01), R1 = make_float2(r01, r11);
+  const float2 Kx = fma2(bc2(s.c10), R1, mul2(bc2(s.c00), R0));  // (K0, K1)
+  const float2 Ky = fma2(bc2(s.c11), R1, mul2(bc2(s.c10), R0));  // (K2, K3)
+  const float2 Ki = fma2(bc2(s.c31), R1, mul2(bc2(s.c30), R0));  // (K6, K7)
+  const float2 Kp = fma2(bc2(s.c41), R1, mul2(bc2(s.c40), R0));  // (K8, K9)
+  const float2 Kt = fma2(bc2(s.c51), R1, mul2(bc2(s.c50), R0));  // (K10, K11)
+  const float res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
+  acc_update(s.x, hx, res0, Kx.x * res0 + Kx.y * res1);
+  acc_update(s.y, hy, res1, Ky.x * res0 + Ky.y * res1);
+  const float dphi = Kp.x * res0 + Kp.y * res1;
+  const float dth = Kt.x * res0 + Kt.y * res1;
+  acc_add(s.phi, dphi);
+  s.theta = s.theta + dth;
+  rotate(s.cP, s.sP, dphi);
+  rotate(s.cT, s.sT, dth);
+  s.ipt = s.ipt + Ki.x * res0 + Ki.y * res1;
+  const float2 P0 = make_float2(s.c00, s.c10), Q = make_float2(s.c10, s.c11);
+  const float c30 = s.c30, c31 = s.c31, c40 = s.c40, c41 = s.c41, c50 = s.c50, c51 = s.c51;
+  s.c00 = fmaf(-Kx.y, s.c10, fmaf(-Kx.x, s.c00, s.c00));
+  const float2 Ny = fma2(bc2(-Ky.y), Q, fma2(bc2(-Ky.x), P0, Q));
+  const float2 Ni = fma2(bc2(-Ki.y), Q, fma2(bc2(-Ki.x), P0, make_float2(c30, c31)));
+  const float2 Np = fma2(bc2(-Kp.y), Q, fma2(bc2(-Kp.x), P0, make_float2(c40, c41)));
+  const float2 Nt = fma2(bc2(-Kt.y), Q, fma2(bc2(-Kt.x), P0, make_float2(c50, c51)));
+  s.c10 = Ny.x; s.c11 = Ny.y;
+  s.c30 = Ni.x; s.c31 = Ni.y;
+  s.c40 = Np.x; s.c41 = Np.y;
+  s.c50 = Nt.x; s.c51 = Nt.y;
+  s.c33 = fmaf(-Ki.y, c31, fmaf(-Ki.x, c30, s.c33));
+  s.c43 = fmaf(-Kp.y, c31, fmaf(-Kp.x, c30, s.c43));
+  s.c44 = fmaf(-Kp.y, c41, fmaf(-Kp.x, c40, s.c44));
+  s.c53 = fmaf(-Kt.y, c31, fmaf(-Kt.x, c30, s.c53));
+  s.c54 = fmaf(-Kt.y, c41, fmaf(-Kt.x, c40, s.c54));
+  s.c55 = fmaf(-Kt.y, c51, fmaf(-Kt.x, c50, s.c55));
+}
+
 template <typename T, typename A, int FORM>
 __device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r11, T hx, T hy) {
+  if constexpr (P2Z_PACKED_F32X2 && FORM == FORM_PRECISE && std::is_same<T, float>::value) {
+    update_v2_apply_packed(s, r00, r01, r11, hx, hy);
+    return;
+  }
   const T K0 = s.c00 * r00 + s.c10 * r01, K1 = s.c00 * r01 + s.c10 * r11;
   const T K2 = s.c10 * r00 + s.c11 * r01, K3 = s.c10 * r01 + s.c11 * r11;
   const T K6 = s.c30 * r00 + s.c31 * r01, K7 = s.c30 * r01 + s.c31 * r11;
