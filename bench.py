@@ -5,7 +5,7 @@ Workload (one GPU): 1000 events x 9600 tracks, 20 layers, FP32, bsize-32
 AOSOA -- the physics workload (charge +-1, pT log-uniform 0.5-20 GeV, phi
 uniform, eta 1.6-2.5, vertex z ~ N(0, 5 cm), correlated PD covariances, hits on
 20 planes z = 30..270 cm at the true helix point plus 30 um / 1 um noise),
-generated from a fixed seed.  A step is one pass of the hot path over all 9.6M
+generated from a fixed seed on the device (p2z_generate_physics_device).  A step is one pass of the hot path over all 9.6M
 tracks x 20 layers.  Inputs (8.1 GB) are larger than L2, so no flush is needed.
 
   value   device-resident throughput (p2z_run_device, CUDA events on the stream)
@@ -397,11 +397,20 @@ def main():
     cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule=args.schedule,
                           block_threads=args.block)
     params = p2z.physics_params(seed=20240601 + rank)
-    trk, hit = p2z.generate_physics(cfg, params)
+    nb = p2z.num_batches(cfg)
+    trk_shape, hit_shape = (nb, p2z.TRK_WORDS, 32), (nb, 20, p2z.HIT_WORDS, 32)
+    # the physics sample generated where it is consumed (p2z_generate_physics_device:
+    # the host generator's per-slot code on the GPU)
+    dt = torch.empty(trk_shape, dtype=torch.float32, device="cuda")
+    dh = torch.empty(hit_shape, dtype=torch.float32, device="cuda")
+    ctx.generate_physics_device(cfg, dt, dh, params=params)
     updates = nev * 9600 * 20
-    dt = torch.from_numpy(trk).cuda()
-    dh = torch.from_numpy(hit).cuda()
     do = torch.empty_like(dt)
+    # host copy of the first events for the CPU baseline (rank 0)
+    n_cpu_ev = 50
+    cpu_sample = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu_sample = (dt[:n_cpu_ev * 300].cpu().numpy(), dh[:n_cpu_ev * 300].cpu().numpy())
 
     def step(c=cfg):
         rc = p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), dt.data_ptr(), dh.data_ptr(), None, do.data_ptr(),
@@ -443,11 +452,11 @@ def main():
     # e2e: host buffers through p2z_run
     e2e = None
     if not args.no_e2e:
-        pin_t = p2z.PinnedArray(trk.shape)
-        pin_h = p2z.PinnedArray(hit.shape)
-        pin_o = p2z.PinnedArray(trk.shape)
-        pin_t.array[...] = trk
-        pin_h.array[...] = hit
+        pin_t = p2z.PinnedArray(trk_shape)
+        pin_h = p2z.PinnedArray(hit_shape)
+        pin_o = p2z.PinnedArray(trk_shape)
+        torch.from_numpy(pin_t.array).copy_(dt)
+        torch.from_numpy(pin_h.array).copy_(dh)
         del dt, dh, do
         torch.cuda.empty_cache()
         ecfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat")
@@ -476,12 +485,14 @@ def main():
     if not args.no_uneven:
         counts = uneven_counts(2000, 77 + rank)
         ucfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20)
-        ut, uh, um = p2z.generate_physics(ucfg, p2z.physics_params(seed=99 + rank), with_mask=True)
-        p2z.mask_layers(um, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=5 + rank)
-        u_upd = int(np.unpackbits(um.view(np.uint8)).sum())
-        udt, udh = torch.from_numpy(ut).cuda(), torch.from_numpy(uh).cuda()
+        unb = p2z.num_batches(ucfg)
+        udt = torch.empty((unb, p2z.TRK_WORDS, 32), dtype=torch.float32, device="cuda")
+        udh = torch.empty((unb, 20, p2z.HIT_WORDS, 32), dtype=torch.float32, device="cuda")
+        udm = torch.empty(unb * 32, dtype=torch.int32, device="cuda")
+        ctx.generate_physics_device(ucfg, udt, udh, udm, params=p2z.physics_params(seed=99 + rank))
+        ctx.mask_layers_device(udm, unb * 32, 20, min_hits=5, max_hits=20, drop_prob=0.1, seed=5 + rank)
         udo = torch.empty_like(udt)
-        udm = torch.from_numpy(um.view(np.int32)).cuda()
+        u_upd = int(ctx.run_device(ucfg, udt, udh, udo, d_mask=udm).updates)
         res, blocks = {}, {"persistent": 128, "per_event": 128}
         tune_uneven = None
         if not args.no_tune:
@@ -565,8 +576,8 @@ def main():
         "serving": serving,
         "outputs_finite": out_ok,
     }
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p2z, trk, hit)
+    if cpu_sample is not None:
+        line["cpu_baseline"] = cpu_baseline(p2z, *cpu_sample)
     print(json.dumps(line))
     ctx.close()
     if world > 1:
