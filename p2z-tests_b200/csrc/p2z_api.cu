@@ -14,6 +14,12 @@
 #include "p2z.h"
 #include "p2z_kernels.cuh"
 
+// p2z_run: the host<->device copies and the kernels are pipelined over at most
+// this many chunks (alternating between two streams).
+#ifndef P2Z_RUN_MAX_CHUNKS
+#define P2Z_RUN_MAX_CHUNKS 8
+#endif
+
 namespace p2z {
 cudaError_t launch_step(int bsize, float *trk, const float *hits, int64_t nslots, int nlayer, int layer, int what,
                         float kfact, cudaStream_t st);
@@ -638,7 +644,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
   // Only the 2-D updates read just the first 6 of the 9 hit words.
   const bool six = (pl.upd == UPDK_V2 || pl.upd == UPDK_V2_COMP || pl.upd == UPDK_F64 || pl.upd == UPDK_V2_REF) &&
                    !(pl.flags & P2Z_FLAG_FULL_HITS);
-  const int64_t nchunk = per_event ? 1 : std::max<int64_t>(1, std::min<int64_t>(8, pl.nbatches / 64));
+  const int64_t nchunk = per_event ? 1 : std::max<int64_t>(1, std::min<int64_t>(P2Z_RUN_MAX_CHUNKS, pl.nbatches / 64));
   const int64_t cb = nchunk ? (pl.nbatches + nchunk - 1) / nchunk : 0;
   int launches = 0;
   int64_t h2d = 0, d2h = 0;
