@@ -413,3 +413,51 @@ def test_staged_schedule_rejects_other_layouts(p2z, ctx):
     with pytest.raises(p2z.P2zError) as e:
         ctx.run_device(cfg, dt, dh, torch.empty_like(dt))
     assert e.value.status == p2z.UNSUPPORTED
+
+
+# ---------------------------------------------------------------------------
+# edge cases: empty runs, layer-count extremes
+# ---------------------------------------------------------------------------
+
+def test_empty_runs(p2z, ctx):
+    """No tracks at all (no events, or only empty events): every entry point
+    returns OK, launches nothing and counts no update."""
+    import torch
+    x = torch.zeros(64).cuda()
+    for cfg in (p2z.make_config(bsize=32, nevts=0, ntrks=9600, nlayer=20),
+                p2z.make_config(bsize=32, nevts=3, event_ntrks=[0, 0, 0], nlayer=20)):
+        for sched in ("flat", "persistent", "per_event", "staged"):
+            cfg.schedule = p2z.SCHED_NAMES[sched]
+            st = ctx.run_device(cfg, x, x, x)
+            assert st.updates == 0 and st.launches == 0
+            st = ctx.run(cfg, np.zeros(1, np.float32), np.zeros(1, np.float32), np.zeros(1, np.float32))
+            assert st.updates == 0
+        best, rows = ctx.autotune(cfg, x, x)
+        assert rows == [] and best["ms"] == 0.0
+        assert p2z.lib.p2z_run_device_noalloc(p2z.C.byref(cfg), None, None, None, None, None) == p2z.OK
+    v = ctx.validate_device(x, 32, 0, 0, [1.0, 1.0, 1.0])
+    assert v.ngood == 0 and v.nnans == 0
+
+
+@pytest.mark.parametrize("nlayer", [1, 32])
+def test_layer_count_extremes(p2z, oracle, ctx, nlayer):
+    """One layer (only the general first step) and 32 layers (every mask bit,
+    including bit 31), unmasked and masked: the precise form against FP64 and
+    the reference-rounding form bit for bit against its restatement."""
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=320, nlayer=nlayer)
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    assert m.max() == (0xFFFFFFFF if nlayer == 32 else 1)
+    out, st = run(p2z, ctx, t, h, 2)
+    assert st.updates == 2 * 320 * nlayer
+    o64 = oracle.run_f64(t, h)
+    g = p2z.tracks_to_aos(out)
+    assert par_rel(g["par"], o64[:, :6]).max() <= PREC_PAR
+    if nlayer == 32:
+        p2z.mask_layers(m, 32, min_hits=5, max_hits=32, drop_prob=0.1, seed=3)
+        assert (m >> 31).max() == 1  # some track keeps its 32nd layer
+    outm, stm = run(p2z, ctx, t, h, 2, mask=m)
+    assert stm.updates == sum(bin(int(x)).count("1") for x in m)
+    o64m = oracle.run_f64(t, h, mask=m)
+    assert par_rel(p2z.tracks_to_aos(outm)["par"], o64m[:, :6]).max() <= PREC_PAR
+    ref, _ = run(p2z, ctx, t, h, 2, mask=m, flags=p2z.FLAG_REFERENCE_ROUNDING)
+    assert _bitdiff(ref, oracle.run_f32(t, h, mask=m, cr_trig=True)) == 0
