@@ -127,8 +127,9 @@ typedef enum p2z_layout {
                                        operation separately rounded, with correctly rounded
                                        sin/cos -- the reference's results bit for bit where its
                                        C library's sinf/cosf are correctly rounded.  Default: the
-                                       precise evaluation (versine form, wide x/y/phi
-                                       accumulators), within ~1e-6 of an FP64 evaluation. */
+                                       precise evaluation (versine form, positions anchored
+                                       at the last hit, carried direction cosines, all FP32),
+                                       within 1e-5 of an FP64 evaluation. */
 
 typedef struct p2z_config {
   int32_t abi_version;   /* must be P2Z_ABI_VERSION */

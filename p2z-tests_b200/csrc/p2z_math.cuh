@@ -18,9 +18,10 @@
 //     (sagitta) signal and the subtraction in FP32 loses most of its digits,
 //     which the reference's FP32 build turns into ~1e-4 relative error in q/pT
 //     and ~1e-3 in the covariance.
-//   * x, y and phi are carried as accumulators wider than FP32 (FP64, or a
-//     float pair in the FP64-free variant): positions of tens of cm held in
-//     FP32 round at ~4e-6 cm, which against 30 um hits biases the curvature.
+//   * x and y are carried as anchored positions (the last hit's coordinate,
+//     exact, plus an FP32 offset) -- or as float pairs, or in FP64 for the
+//     all-FP64 kernel: positions of tens of cm held in FP32 round at ~4e-6 cm,
+//     which against 30 um hits biases the curvature.
 // FORM_REFERENCE: the reference's FP32 evaluation operation for operation,
 //   including its C type promotions (the double literals in `1./ipt`,
 //   `1.0/cosT`, `(1.-cosa)` ... and the double determinant), for callers who
@@ -80,7 +81,11 @@ __device__ __forceinline__ void acc_set(DF &a, float v) { a.hi = v; a.lo = 0.f; 
 __device__ __forceinline__ void acc_set(AP &a, float v) { a.a = v; a.u = 0.f; }
 __device__ __forceinline__ void acc_add(AP &a, float d) { a.u += d; }
 
-__device__ __forceinline__ void acc_add(float &a, float d) { a = a + d; }
+// A float accumulator adds with an explicit rounding: an increment that is also
+// used elsewhere (the helix angle, the Kalman corrections of phi and theta) must
+// not be fused into the addition in one kernel and not in another, so that
+// every schedule computes the same bits.
+__device__ __forceinline__ void acc_add(float &a, float d) { a = __fadd_rn(a, d); }
 __device__ __forceinline__ void acc_add(double &a, float d) { a += (double)d; }
 __device__ __forceinline__ void acc_add(double &a, double d) { a += d; }
 __device__ __forceinline__ void acc_add(DF &a, float d) {
@@ -207,15 +212,17 @@ __device__ __forceinline__ void rotate(float &c, float &s, float d) {
 // T: element type of the bulk arithmetic; A: type of the x, y, phi accumulators.
 // Covariance: the 15 live elements, named by (row, column); packed indices in
 // comments.
-// phi is carried in a wide float when the positions are anchored (AP): it has
-// no natural anchor, and it is only an output (its cos/sin are rotated).
+// With anchored positions (AP) phi is a plain float: it has no natural anchor,
+// it is only an output (the propagation uses the carried cos/sin of phi, which
+// are rotated), and its 40 roundings per track stay below 1.4e-6 rad on the
+// 9.6M-track physics workload -- so the default form uses no FP64 at all.
 template <typename A>
 struct PhiOf {
   using type = A;
 };
 template <>
 struct PhiOf<AP> {
-  using type = double;
+  using type = float;
 };
 
 template <typename T, typename A>
@@ -585,7 +592,7 @@ __device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r
   const float dphi = Kp.x * res0 + Kp.y * res1;
   const float dth = Kt.x * res0 + Kt.y * res1;
   acc_add(s.phi, dphi);
-  s.theta = s.theta + dth;
+  s.theta = __fadd_rn(s.theta, dth);
   rotate(s.cP, s.sP, dphi);
   rotate(s.cT, s.sT, dth);
   s.ipt = s.ipt + Ki.x * res0 + Ki.y * res1;
@@ -632,7 +639,7 @@ __device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r1
     const float dphi = K8 * res0 + K9 * res1;
     const float dth = K10 * res0 + K11 * res1;
     acc_add(s.phi, dphi);
-    s.theta = s.theta + dth;
+    s.theta = __fadd_rn(s.theta, dth);
     rotate(s.cP, s.sP, dphi);
     rotate(s.cT, s.sT, dth);
   } else {

@@ -341,13 +341,24 @@ def test_nonfinite_inputs_propagate_like_reference(p2z, oracle, ctx, physics):
 def test_full_size_properties(p2z, oracle, ctx):
     import torch
     cfg = p2z.make_config(bsize=32, nevts=1000, ntrks=9600, nlayer=20)
-    trk, hit = p2z.generate_physics(cfg)
-    dt, dh = torch.from_numpy(trk).cuda(), torch.from_numpy(hit).cuda()
+    nb = p2z.num_batches(cfg)
+    dt = torch.empty((nb, 28, 32), device="cuda")
+    dh = torch.empty((nb, 20, 9, 32), device="cuda")
+    ctx.generate_physics_device(cfg, dt, dh)
     do = torch.empty_like(dt)
     st = ctx.run_device(cfg, dt, dh, do)
     assert st.singular == 0 and st.updates == 9600 * 1000 * 20
-    out = do.cpu().numpy()
-    del dt, dh, do
+    # every one of the 9.6M tracks against the FP64 kernel (itself pinned to the FP64 oracle)
+    ref = torch.empty_like(dt)
+    cfg.update = p2z.UPDATE_F64
+    ctx.run_device(cfg, dt, dh, ref)
+    p, r = do.permute(0, 2, 1).reshape(-1, 28).double(), ref.permute(0, 2, 1).reshape(-1, 28).double()
+    floor = torch.tensor([1.0, 1.0, 1.0, 1e-3, 1.0, 1e-2], dtype=torch.float64, device="cuda")
+    prel = ((p[:, :6] - r[:, :6]).abs() / torch.maximum(r[:, :6].abs(), floor)).max(0).values.cpu().numpy()
+    print("9.6M tracks, precise v2 vs FP64 kernel: par max", prel)
+    assert prel.max() <= PREC_PAR
+    out, trk, hit = do.cpu().numpy(), dt.cpu().numpy(), dh.cpu().numpy()
+    del dt, dh, do, ref, p, r
     g = p2z.tracks_to_aos(out)
     a = p2z.tracks_to_aos(trk)
     hh_last = hit[:, 19, 2, :].reshape(-1)
