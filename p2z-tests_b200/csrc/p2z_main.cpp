@@ -8,7 +8,10 @@
 // usage: p2z_main SEEDFILE [nevts ntrks bsize nlayer niter [smear [cov_scale]]]
 // SEEDFILE: first line 6 track parameters, 21 covariance elements and the
 // charge; then one line per layer with 3 hit positions and 6 covariance
-// elements (layer order).
+// elements (layer order).  The environment variable P2Z_FLAGS (an integer,
+// decimal or 0x-hex) sets p2z_config.flags, e.g. P2Z_FLAGS=0x20 for the
+// reference's own rounding (P2Z_FLAG_REFERENCE_ROUNDING); P2Z_UPDATE selects the
+// update kind (p2z_update_kind, default 0 = KalmanUpdate_v2).
 #include <sys/time.h>
 
 #include <chrono>
@@ -82,6 +85,8 @@ int main(int argc, char **argv) {
   cfg.ntrks = ntrks;
   cfg.nlayer = nlayer;
   cfg.niter = niter;
+  if (const char *fl = std::getenv("P2Z_FLAGS")) cfg.flags = (uint32_t)std::strtoul(fl, nullptr, 0);
+  if (const char *up = std::getenv("P2Z_UPDATE")) cfg.update = (int32_t)std::strtol(up, nullptr, 0);
   const int64_t nb = p2z_num_batches(&cfg);
   if (nb < 0) {
     std::fprintf(stderr, "bad sizes: %s\n", p2z_last_error(nullptr));

@@ -15,7 +15,7 @@ Tolerances (stated here, derived from the oracle comparison):
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, LIVE, cov_rel, par_rel
+from conftest import GOLDEN, LIVE, ROOT, cov_rel, par_rel
 
 pytestmark = pytest.mark.gpu
 
@@ -472,3 +472,35 @@ def test_layer_count_extremes(p2z, oracle, ctx, nlayer):
     assert par_rel(p2z.tracks_to_aos(outm)["par"], o64m[:, :6]).max() <= PREC_PAR
     ref, _ = run(p2z, ctx, t, h, 2, mask=m, flags=p2z.FLAG_REFERENCE_ROUNDING)
     assert _bitdiff(ref, oracle.run_f32(t, h, mask=m, cr_trig=True)) == 0
+
+
+def test_driver_reproduces_the_reference_printout(p2z):
+    """The C++ driver (p2z_main: prepare, p2z_run from pinned host memory,
+    validation, the reference's printed lines) on the known-answer input with
+    the reference's own rounding prints the golden block of
+    logs/propagate_gcc_omp.log:30-40 (the last printed digit of pt may differ by
+    one, as between the reference's own builds) and a "formatted" line that
+    the reference's tools parse (tools/compare.py:12 reads it positionally)."""
+    import json
+    import os
+    import subprocess
+    exe = ROOT / "p2z-tests_b200" / "p2z_main"
+    meta = json.loads((GOLDEN / "kat_block.json").read_text())
+    gold = meta["blocks"]["propagate_gcc_omp.log"]
+    env = dict(os.environ, P2Z_FLAGS="0x20")
+    r = subprocess.run([str(exe), str(GOLDEN / "kat_seed.txt"), "100", "9600", "32", "20", "1"], capture_output=True,
+                       text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    fmt = next(l for l in lines if l.startswith("formatted "))
+    f = fmt.split()
+    assert f[1:6] == ["1", "100", "9600", "32", "300"] and float(f[6]) > 0
+    vals = {}
+    for l in lines:
+        if l.startswith("track ") and "avg=" in l:
+            name = l.split()[1].split("/")[0]
+            vals[name] = l.split("avg=")[1].split()[0]
+    assert lines[-1] == "number of tracks failed=0"
+    for k in ("x", "y", "z", "dx", "dy", "pt", "phi", "theta"):
+        want = gold[k][0] if isinstance(gold[k], list) else gold[k]
+        assert abs(float(vals[k]) - float(want)) <= 1.5e-6, (k, vals[k], want)
