@@ -267,13 +267,15 @@ def run_serving(p2z, device, rank, args):
         pool.append((t, h, m, o, int(n)))
     out = {"workload": "events of 1k-20k tracks (log-uniform), 20 layers, 5-20 hits/track with 10% dropped, "
                        "3x3 update with FP64 inversion + Joseph, Poisson arrivals",
-           "device_budget_gb": 40, "events_per_rate": args.serve_events, "rates": []}
+           "device_budget_gb": 40, "events_per_rate": args.serve_events, "groups_in_flight": args.serve_inflight,
+           "rates": []}
     with p2z.Server(device=device, bsize=32, nlayer=20, update="3x3_f64", budget_bytes=40 << 30,
-                    max_inflight=2) as srv:
+                    max_inflight=args.serve_inflight) as srv:
         # warm-up
         srv.replay([(e[0].array, e[1].array, e[2].array, e[4], e[3].array) for e in pool[:16]],
                    np.zeros(16))
-        for rate in SERVE_RATES:
+        rates = [int(r) for r in args.serve_rates.split(",")] if args.serve_rates else SERVE_RATES
+        for rate in rates:
             n = args.serve_events
             idx = rng.integers(0, npool, n)
             arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
@@ -373,6 +375,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-events", type=int, default=1500)
+    ap.add_argument("--serve-inflight", type=int, default=8, help="server groups in flight (1..8)")
+    ap.add_argument("--serve-rates", default="", help="comma-separated offered rates (events/s); default sweep")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "flat", "persistent", "per_event", "staged"],
                     help="launch schedule of the headline step (auto: what the autotuner measured best)")
