@@ -69,3 +69,34 @@ def test_replay_reports_latencies(p2z, ctx):
     assert (lat > 0).all() and (lat < 30).all()
     assert all(i.admit_s >= i.submit_s and i.launch_s >= i.admit_s and i.done_s >= i.launch_s for i in infos)
     assert sum(i.updates for i in infos) == sum(int(np.unpackbits(e[2].view(np.uint8)).sum()) for e in evs)
+
+
+def test_poll_wait_timeout_and_release(p2z):
+    """A request that cannot have finished (its inputs are still being
+    copied) reports NOT_READY to poll and TIMEOUT to a wait that has already
+    run out; waiting completes it; a reported request is released, and an
+    unknown id is an error."""
+    n = 300000
+    cfg = p2z.make_config(bsize=32, nevts=1, event_ntrks=[n], nlayer=20)
+    nb = p2z.num_batches(cfg)
+    t, h, o = p2z.PinnedArray((nb, 28, 32)), p2z.PinnedArray((nb, 20, 9, 32)), p2z.PinnedArray((nb, 28, 32))
+    try:
+        p2z.generate_physics(cfg, out=(t.array, h.array, None))
+        with p2z.Server(bsize=32, nlayer=20, budget_bytes=2 << 30) as srv:
+            rid = srv.submit(t.array, h.array, None, n, o.array)
+            assert srv.poll(rid) is None  # 216 MB of hits cannot have crossed the bus yet
+            with pytest.raises(p2z.P2zError) as e:
+                srv.wait(rid, timeout=1e-9)
+            assert e.value.status == p2z.TIMEOUT
+            info = srv.wait(rid, timeout=600.0)
+            assert info.status == p2z.OK and info.ntrks == n and info.updates == n * 20
+            assert info.submit_s <= info.admit_s <= info.launch_s <= info.done_s
+            with pytest.raises(p2z.P2zError) as e:   # released once reported
+                srv.poll(rid)
+            assert e.value.status == p2z.BAD_ARG
+            with pytest.raises(p2z.P2zError) as e:
+                srv.wait(10 ** 9, timeout=1.0)
+            assert e.value.status == p2z.BAD_ARG
+        assert np.isfinite(o.array[:, :6, :]).all()
+    finally:
+        t.free(); h.free(); o.free()
