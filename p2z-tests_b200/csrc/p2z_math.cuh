@@ -156,14 +156,13 @@ __device__ __forceinline__ void sv_series(float a, float *s, float *v) {
   *v = a2 * pv;
 }
 
-// The same for the small Kalman corrections of phi and theta, to a^5/5! and
-// a^6/6! (truncation below 1e-9 relative for |a| <= 0.2, 1.6e-6 at |a| = 0.5).
-__device__ __forceinline__ void sv_series_short(float a, float *s, float *v) {
+// The same for the theta offset, which only sums Kalman corrections (of order
+// 1e-3 rad): sin(a) = a - a^3/3!, 1 - cos(a) = a^2/2!, truncation below
+// a^5/5! and a^4/4! -- under 3e-11 and 7e-9 absolute for |a| <= 0.02.
+__device__ __forceinline__ void sv_series_tiny(float a, float *s, float *v) {
   const float a2 = a * a;
-  const float ps = fmaf(a2, 8.3333333e-3f, -1.6666667e-1f);
-  *s = fmaf(a * a2, ps, a);
-  const float pv = fmaf(a2, 1.3888889e-3f, -4.1666667e-2f);
-  *v = a2 * fmaf(a2, pv, 0.5f);
+  *s = fmaf(a * a2, -1.6666667e-1f, a);
+  *v = 0.5f * a2;
 }
 
 // sin(a) and 1 - cos(a) without cancellation.
@@ -192,19 +191,21 @@ __device__ __forceinline__ void sincos_angle(float a, float *s, float *c) {
 __device__ __forceinline__ float sinf_cr(float x) { return (float)sin((double)x); }
 __device__ __forceinline__ float cosf_cr(float x) { return (float)cos((double)x); }
 
-// Rotate the unit vector (c, s) = (cos t, sin t) to t + d:
-// cos(t+d) = c - (c*v + s*w), sin(t+d) = s - (s*v - c*w) with w = sin d and
-// v = 1 - cos d from their short series (sv_series_short).  No branch: Kalman
-// corrections to phi and theta are far below 0.2 rad for any track the filter
-// can follow, and NaN or Inf propagate.
-__device__ __forceinline__ void rotate(float &c, float &s, float d) {
-  float w, v;
-  sv_series_short(d, &w, &v);
-  const float cn = c - fmaf(c, v, s * w);
-  const float sn = s - fmaf(s, v, -(c * w));
-  c = cn;
-  s = sn;
+// The unit vector (c, s) = (cos t, sin t) rotated to t + d, given w = sin d
+// and v = 1 - cos d: cos(t+d) = c - (c*v + s*w), sin(t+d) = s - (s*v - c*w).
+// (Scalar: as packed pairs the register-pair moves cost more than they save.)
+__device__ __forceinline__ void rotated(float c, float s, float w, float v, float *cn, float *sn) {
+  *cn = c - fmaf(c, v, s * w);
+  *sn = s - fmaf(s, v, -(c * w));
 }
+
+// Re-anchoring thresholds of the carried phi and theta offsets.  After a
+// propagation |dP| <= 0.4, so the next step evaluates its phi offset (plus
+// that step's Kalman correction, of order 1e-3 rad) inside the 0.5 rad range
+// of sv_series; |dT| <= 0.02 keeps the theta offset inside the range of
+// sv_series_tiny.
+constexpr float kAnchorPhi = 0.4f;
+constexpr float kAnchorTheta = 0.02f;
 
 // ---------------------------------------------------------------------------
 // Track state in registers
@@ -212,10 +213,10 @@ __device__ __forceinline__ void rotate(float &c, float &s, float d) {
 // T: element type of the bulk arithmetic; A: type of the x, y, phi accumulators.
 // Covariance: the 15 live elements, named by (row, column); packed indices in
 // comments.
-// With anchored positions (AP) phi is a plain float: it has no natural anchor,
-// it is only an output (the propagation uses the carried cos/sin of phi, which
-// are rotated), and its 40 roundings per track stay below 1.4e-6 rad on the
-// 9.6M-track physics workload -- so the default form uses no FP64 at all.
+// With anchored positions (AP) phi is a plain float: it is only an output (the
+// propagation uses the anchored direction below), and its 40 roundings per
+// track stay below 1.5e-6 relative on the 9.6M-track physics workload -- so
+// the default form uses no FP64 at all.
 template <typename A>
 struct PhiOf {
   using type = A;
@@ -230,10 +231,15 @@ struct Trk {
   A x, y;
   typename PhiOf<A>::type phi;
   T z, ipt, theta;
-  // FORM_PRECISE carries cos/sin of phi and theta from layer to layer and
-  // rotates them by each step's angle increment (alpha in the propagation, the
-  // Kalman corrections in the update) instead of evaluating sin/cos anew.
+  // FORM_PRECISE: (cP, sP) and (cT, sT) are an anchor direction -- cos/sin of
+  // phi and theta at some earlier point of the track -- and dP, dT the angle
+  // increments summed since then (alpha in the propagation, the Kalman
+  // corrections in the update).  The direction a step uses is the anchor
+  // rotated once by the offset, so the rounding of a rotation enters one
+  // step only instead of accumulating over the track; the anchor moves
+  // (re-anchoring) only when an offset outgrows its series' range.
   T cP, sP, cT, sT;
+  T dP, dT;
   T c00, c10, c11;            // 0 1 2
   T c30, c31, c33;            // 6 7 9
   T c40, c41, c43, c44;       // 10 11 13 14
@@ -274,15 +280,39 @@ struct Jac {
 // the series of sv_series with no range branch: |cosP*sina| <= 1, where the
 // series' truncation is below 3.3e-6 relative (sin) and 6.1e-7 (versine) --
 // far inside what the covariance needs -- and below 1e-8 for |a| <= 0.5.
+//
+// The direction: (cosP, sinP) and (cos, sin) of theta are the anchors rotated
+// by the offsets dP and dT.  Afterwards dP advances by alpha; when that takes
+// it past kAnchorPhi the anchor moves to the direction after the step
+// (rotated from (cosP, sinP) by alpha with sina and omc) and dP restarts at 0.
+// A theta offset past kAnchorTheta (the Kalman corrections of a diverging
+// track) moves the theta anchor to this step's direction.  Selects, no branch.
 template <int SC, typename A>
 __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
   Helix<float> h;
   h.deltaZ = zout - s.z;
   h.pt = rcp_nr(s.ipt);
-  h.cosP = s.cP;
-  h.sinP = s.sP;
-  const float icosT = rcp_nr(s.cT);
-  h.tanT = s.sT * icosT;
+  {
+    // SC_FAST: |dP| <= kAnchorPhi + one Kalman correction, inside the series'
+    // range, so no range branch (a branch would end the basic block and keep
+    // the scheduler from overlapping this with the previous update)
+    float w, v;
+    if (SC == SC_FAST) sv_series(s.dP, &w, &v);
+    else sin_versine<SC>(s.dP, &w, &v);
+    rotated(s.cP, s.sP, w, v, &h.cosP, &h.sinP);
+  }
+  float cosT, sinT;
+  {
+    float w, v;
+    sv_series_tiny(s.dT, &w, &v);
+    rotated(s.cT, s.sT, w, v, &cosT, &sinT);
+  }
+  const bool moveT = fabsf(s.dT) > kAnchorTheta;
+  s.cT = moveT ? cosT : s.cT;
+  s.sT = moveT ? sinT : s.sT;
+  s.dT = moveT ? 0.f : s.dT;
+  const float icosT = rcp_nr(cosT);
+  h.tanT = sinT * icosT;
   h.icT2 = icosT * icosT;
   h.dzk = (SC == SC_FAST) ? h.deltaZ * ik : __fdiv_rn(h.deltaZ, k);
   const float alpha = (h.dzk * h.tanT) * s.ipt;
@@ -297,17 +327,33 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   acc_add(s.phi, alpha);
   if (SC == SC_FAST) sv_series(h.m1, &h.sCPs, &h.omcC);
   else sin_versine<SC>(h.m1, &h.sCPs, &h.omcC);
-  // phi advanced by alpha: rotate (cos phi, sin phi) with sin(alpha) and the versine
-  s.cP = h.cosP - fmaf(h.cosP, h.omc, h.m2);
-  s.sP = h.sinP - fmaf(h.sinP, h.omc, -h.m1);
+  const float dP = __fadd_rn(s.dP, alpha);
+  const bool moveP = fabsf(dP) > kAnchorPhi;
+  // (cos, sin) of phi + alpha from sin(alpha) and the versine
+  const float cPn = h.cosP - fmaf(h.cosP, h.omc, h.m2);
+  const float sPn = h.sinP - fmaf(h.sinP, h.omc, -h.m1);
+  s.cP = moveP ? cPn : s.cP;
+  s.sP = moveP ? sPn : s.sP;
+  s.dP = moveP ? 0.f : dP;
   return h;
 }
 
-// First evaluation of the carried direction cosines of a track.
+// First evaluation of the carried direction of a track: the anchors at the
+// input angles, zero offsets.
 template <typename A>
 __device__ __forceinline__ void init_direction(Trk<float, A> &s) {
   sincosf(tof(s.phi), &s.sP, &s.cP);
   sincosf(s.theta, &s.sT, &s.cT);
+  s.dP = 0.f;
+  s.dT = 0.f;
+}
+
+// A Kalman correction of phi and theta, added to the offsets from the
+// anchors (the output angles accumulate it separately).
+template <typename A>
+__device__ __forceinline__ void turn_direction(Trk<float, A> &s, float dphi, float dth) {
+  s.dP = __fadd_rn(s.dP, dphi);
+  s.dT = __fadd_rn(s.dT, dth);
 }
 
 // The Jacobian entries (reference :655-666) with the shared factors taken out
@@ -593,8 +639,7 @@ __device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r
   const float dth = Kt.x * res0 + Kt.y * res1;
   acc_add(s.phi, dphi);
   s.theta = __fadd_rn(s.theta, dth);
-  rotate(s.cP, s.sP, dphi);
-  rotate(s.cT, s.sT, dth);
+  turn_direction(s, dphi, dth);
   s.ipt = s.ipt + Ki.x * res0 + Ki.y * res1;
   const float2 P0 = make_float2(s.c00, s.c10), Q = make_float2(s.c10, s.c11);
   const float c30 = s.c30, c31 = s.c31, c40 = s.c40, c41 = s.c41, c50 = s.c50, c51 = s.c51;
@@ -640,8 +685,7 @@ __device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r1
     const float dth = K10 * res0 + K11 * res1;
     acc_add(s.phi, dphi);
     s.theta = __fadd_rn(s.theta, dth);
-    rotate(s.cP, s.sP, dphi);
-    rotate(s.cT, s.sT, dth);
+    turn_direction(s, dphi, dth);
   } else {
     acc_add(s.x, K0 * res0 + K1 * res1);
     acc_add(s.y, K2 * res0 + K3 * res1);
@@ -777,8 +821,7 @@ __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float 
   const float dth = theta_new - s.theta;
   acc_add(s.phi, dphi);
   s.theta = theta_new;
-  rotate(s.cP, s.sP, dphi);
-  rotate(s.cT, s.sT, dth);
+  turn_direction(s, dphi, dth);
   // Joseph form: P = (I - K H) C, C'' = P - P H^T K^T + K V K^T, with
   // P(i,j) = C(i,j) - K(i,0) C(0,j) - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0.
   const U Cm[5][5] = {{C00, C10, C30, C40, C50},

@@ -374,6 +374,66 @@ def test_full_size_properties(p2z, oracle, ctx):
     assert par_rel(gs["par"], o64[:, :6]).max() <= PREC_PAR
 
 
+PREC_PAR_FULL = 5e-6
+
+
+def _float_state_floor(oracle, trk1, hit1):
+    """FP64 oracle one layer at a time with the state rounded to FP32 in
+    between: the error any kernel holding an FP32 state between layers has."""
+    cur = trk1.copy()
+    nb, _, B = trk1.shape
+    for l in range(hit1.shape[1]):
+        o = oracle.run_f64(cur, np.ascontiguousarray(hit1[:, l:l + 1]))
+        cur[:, :27, :] = o.reshape(nb, B, 27).astype(np.float32).transpose(0, 2, 1)
+    return cur
+
+
+@pytest.mark.parametrize("seed", [20240601, 4, 6])
+def test_full_size_precision(p2z, oracle, ctx, seed):
+    """Every one of the 9.6M tracks of the physics workload (three samples)
+    against the FP64 kernel: parameters within 5e-6 relative; live covariance
+    within 1e-4 of sqrt(C_ii C_jj), or within 3x the track's float-state floor
+    where that floor is itself near the bound (an ill-conditioned track whose
+    FP32 state alone costs ~1e-4)."""
+    import torch
+    cfg = p2z.make_config(bsize=32, nevts=1000, ntrks=9600, nlayer=20)
+    nb = p2z.num_batches(cfg)
+    dt = torch.empty((nb, 28, 32), device="cuda")
+    dh = torch.empty((nb, 20, 9, 32), device="cuda")
+    ctx.generate_physics_device(cfg, dt, dh, params=p2z.physics_params(seed=seed))
+    do, ref = torch.empty_like(dt), torch.empty_like(dt)
+    ctx.run_device(cfg, dt, dh, do)
+    cfg.update = p2z.UPDATE_F64
+    ctx.run_device(cfg, dt, dh, ref)
+    p, r = do.permute(0, 2, 1).reshape(-1, 28).double(), ref.permute(0, 2, 1).reshape(-1, 28).double()
+    floor = torch.tensor([1.0, 1.0, 1.0, 1e-3, 1.0, 1e-2], dtype=torch.float64, device="cuda")
+    prel = ((p[:, :6] - r[:, :6]).abs() / torch.maximum(r[:, :6].abs(), floor)).max(0).values.cpu().numpy()
+    diag = [i * (i + 1) // 2 + i for i in range(6)]
+    cerr = []
+    for k in LIVE:
+        i = int((np.sqrt(8 * k + 1) - 1) // 2)
+        j = k - i * (i + 1) // 2
+        s = (r[:, 6 + diag[i]] * r[:, 6 + diag[j]]).abs().sqrt()
+        cerr.append((p[:, 6 + k] - r[:, 6 + k]).abs() / torch.where(s > 0, s, torch.ones_like(s)))
+    cerr = torch.stack(cerr, 1).max(1).values
+    print(f"seed {seed}: par max {prel}, cov max {float(cerr.max()):.2e}")
+    assert prel.max() <= PREC_PAR_FULL
+    over = torch.nonzero(cerr > PREC_COV).flatten().cpu().numpy()
+    assert len(over) <= 8, f"{len(over)} tracks over the covariance bound"
+    for sl in over:
+        b, t = divmod(int(sl), 32)
+        trk1, hit1 = dt[b:b + 1].cpu().numpy(), dh[b:b + 1].cpu().numpy()
+        full = oracle.run_f64(trk1, hit1)[t]
+        fs = _float_state_floor(oracle, trk1, hit1)[0, :27, t].astype(np.float64)
+        got = p[sl].cpu().numpy()
+        for k in LIVE:
+            i = int((np.sqrt(8 * k + 1) - 1) // 2)
+            j = k - i * (i + 1) // 2
+            sc = np.sqrt(abs(full[6 + diag[i]] * full[6 + diag[j]]))
+            err, fl = abs(got[6 + k] - full[6 + k]) / sc, abs(fs[6 + k] - full[6 + k]) / sc
+            assert err <= max(PREC_COV, 3 * fl), (sl, k, err, fl)
+
+
 @pytest.mark.parametrize("update", ["v2", "3x3_f64", "v2_comp", "f64"])
 @pytest.mark.parametrize("masked", [False, True])
 def test_staged_schedule_bitwise_equal(p2z, ctx, update, masked):
