@@ -156,13 +156,19 @@ __device__ __forceinline__ void sv_series(float a, float *s, float *v) {
   *v = a2 * pv;
 }
 
-// The same for the theta offset, which only sums Kalman corrections (of order
-// 1e-3 rad): sin(a) = a - a^3/3!, 1 - cos(a) = a^2/2!, truncation below
-// a^5/5! and a^4/4! -- under 3e-11 and 7e-9 absolute for |a| <= 0.02.
-__device__ __forceinline__ void sv_series_tiny(float a, float *s, float *v) {
-  const float a2 = a * a;
-  *s = fmaf(a * a2, -1.6666667e-1f, a);
-  *v = 0.5f * a2;
+// tan(t + d) from tA = tan(t) and a small offset d (the theta offset, which
+// only sums Kalman corrections of order 1e-3 rad):
+//   tan(t + d) = tA + u (1 + tA^2) / (1 - tA u),  u = tan d = d + d^3/3 + ...,
+// with 1/(1 - x) = 1 + x + x^2 + ... to x^2.  For |d| (1 + |tA|) <= 0.01 the
+// truncations are below 1.4e-11 (u) and 1e-6 of the increment (the quotient,
+// (tA u)^3); the increment is formed first and added to tA last (one rounding
+// at the size of the result).
+__device__ __forceinline__ float tan_offset(float tA, float d) {
+  const float u = fmaf(d * d, d * 0.33333334f, d);
+  const float tu = tA * u;
+  const float q = fmaf(tu, tu, tu);
+  const float r = u * fmaf(tA, tA, 1.f);
+  return tA + fmaf(r, q, r);
 }
 
 // sin(a) and 1 - cos(a) without cancellation.
@@ -202,10 +208,10 @@ __device__ __forceinline__ void rotated(float c, float s, float w, float v, floa
 // Re-anchoring thresholds of the carried phi and theta offsets.  After a
 // propagation |dP| <= 0.4, so the next step evaluates its phi offset (plus
 // that step's Kalman correction, of order 1e-3 rad) inside the 0.5 rad range
-// of sv_series; |dT| <= 0.02 keeps the theta offset inside the range of
-// sv_series_tiny.
+// of sv_series; |dT| (1 + |tan theta|) <= 0.01 keeps the theta offset inside
+// the range of tan_offset.
 constexpr float kAnchorPhi = 0.4f;
-constexpr float kAnchorTheta = 0.02f;
+constexpr float kAnchorTheta = 0.01f;
 
 // ---------------------------------------------------------------------------
 // Track state in registers
@@ -231,14 +237,14 @@ struct Trk {
   A x, y;
   typename PhiOf<A>::type phi;
   T z, ipt, theta;
-  // FORM_PRECISE: (cP, sP) and (cT, sT) are an anchor direction -- cos/sin of
-  // phi and theta at some earlier point of the track -- and dP, dT the angle
-  // increments summed since then (alpha in the propagation, the Kalman
+  // FORM_PRECISE: an anchor direction -- (cP, sP) = cos/sin of phi and
+  // tT = tan(theta) at some earlier point of the track -- and dP, dT the
+  // angle increments summed since then (alpha in the propagation, the Kalman
   // corrections in the update).  The direction a step uses is the anchor
-  // rotated once by the offset, so the rounding of a rotation enters one
-  // step only instead of accumulating over the track; the anchor moves
+  // advanced once by the offset, so the rounding of that evaluation enters
+  // one step only instead of accumulating over the track; the anchor moves
   // (re-anchoring) only when an offset outgrows its series' range.
-  T cP, sP, cT, sT;
+  T cP, sP, tT;
   T dP, dT;
   T c00, c10, c11;            // 0 1 2
   T c30, c31, c33;            // 6 7 9
@@ -281,12 +287,13 @@ struct Jac {
 // series' truncation is below 3.3e-6 relative (sin) and 6.1e-7 (versine) --
 // far inside what the covariance needs -- and below 1e-8 for |a| <= 0.5.
 //
-// The direction: (cosP, sinP) and (cos, sin) of theta are the anchors rotated
-// by the offsets dP and dT.  Afterwards dP advances by alpha; when that takes
-// it past kAnchorPhi the anchor moves to the direction after the step
-// (rotated from (cosP, sinP) by alpha with sina and omc) and dP restarts at 0.
-// A theta offset past kAnchorTheta (the Kalman corrections of a diverging
-// track) moves the theta anchor to this step's direction.  Selects, no branch.
+// The direction: (cosP, sinP) is the phi anchor rotated by dP, tan(theta) the
+// theta anchor advanced by dT, and 1/cos^2(theta) = 1 + tan^2(theta).
+// Afterwards dP advances by alpha; when that takes it past kAnchorPhi the
+// anchor moves to the direction after the step (rotated from (cosP, sinP) by
+// alpha with sina and omc) and dP restarts at 0.  A theta offset past
+// kAnchorTheta moves the theta anchor to this step's tan(theta).  Selects, no
+// branch.
 template <int SC, typename A>
 __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
   Helix<float> h;
@@ -301,19 +308,11 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
     else sin_versine<SC>(s.dP, &w, &v);
     rotated(s.cP, s.sP, w, v, &h.cosP, &h.sinP);
   }
-  float cosT, sinT;
-  {
-    float w, v;
-    sv_series_tiny(s.dT, &w, &v);
-    rotated(s.cT, s.sT, w, v, &cosT, &sinT);
-  }
-  const bool moveT = fabsf(s.dT) > kAnchorTheta;
-  s.cT = moveT ? cosT : s.cT;
-  s.sT = moveT ? sinT : s.sT;
+  h.tanT = tan_offset(s.tT, s.dT);
+  h.icT2 = fmaf(h.tanT, h.tanT, 1.f);
+  const bool moveT = fmaf(fabsf(s.tT), fabsf(s.dT), fabsf(s.dT)) > kAnchorTheta;
+  s.tT = moveT ? h.tanT : s.tT;
   s.dT = moveT ? 0.f : s.dT;
-  const float icosT = rcp_nr(cosT);
-  h.tanT = sinT * icosT;
-  h.icT2 = icosT * icosT;
   h.dzk = (SC == SC_FAST) ? h.deltaZ * ik : __fdiv_rn(h.deltaZ, k);
   const float alpha = (h.dzk * h.tanT) * s.ipt;
   sin_versine<SC>(alpha, &h.sina, &h.omc);
@@ -343,7 +342,9 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
 template <typename A>
 __device__ __forceinline__ void init_direction(Trk<float, A> &s) {
   sincosf(tof(s.phi), &s.sP, &s.cP);
-  sincosf(s.theta, &s.sT, &s.cT);
+  float sT, cT;
+  sincosf(s.theta, &sT, &cT);
+  s.tT = __fdiv_rn(sT, cT);
   s.dP = 0.f;
   s.dT = 0.f;
 }
