@@ -117,9 +117,10 @@ typedef enum p2z_layout {
 #define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan inputs for NaN/Inf first -> P2Z_NONFINITE_INPUT */
 #define P2Z_FLAG_STRICT       0x2u  /* return P2Z_SINGULAR if any det <= 0 was met */
 #define P2Z_FLAG_NO_GRAPH     0x4u  /* PERSISTENT: launch directly instead of replaying a graph */
-#define P2Z_FLAG_ACCURATE_TRIG 0x8u /* sincosf for every angle (default: MUFU sin/cos for phi and
-                                       theta, a Taylor polynomial for the small angles alpha and
-                                       cosP*sina) */
+#define P2Z_FLAG_ACCURATE_TRIG 0x8u /* sin and 1 - cos of every per-layer angle from sincosf of its
+                                       half (default: Taylor polynomials for the helix angle alpha
+                                       when |alpha| <= 0.5, for cosP*sin(alpha) and for the phi
+                                       offset from its anchor; sincosf beyond 0.5 rad) */
 #define P2Z_FLAG_FULL_HITS    0x10u /* p2z_run: copy all 9 hit words per track even for the 2-D
                                        updates (default: only the 6 words they read) */
 #define P2Z_FLAG_REFERENCE_ROUNDING 0x20u /* P2Z_UPDATE_V2 only: evaluate the reference's own FP32
@@ -128,8 +129,9 @@ typedef enum p2z_layout {
                                        sin/cos -- the reference's results bit for bit where its
                                        C library's sinf/cosf are correctly rounded.  Default: the
                                        precise evaluation (versine form, positions anchored
-                                       at the last hit, carried direction cosines, all FP32),
-                                       within 1e-5 of an FP64 evaluation. */
+                                       at the last hit, direction anchored and advanced by
+                                       summed angle offsets, all FP32), within 5e-6 of an FP64
+                                       evaluation. */
 
 typedef struct p2z_config {
   int32_t abi_version;   /* must be P2Z_ABI_VERSION */

@@ -184,14 +184,6 @@ __device__ __forceinline__ void sin_versine(float a, float *s, float *v) {
   }
 }
 
-// Angle phi: MUFU approximation (absolute error ~2^-21 for |x| <= pi) in the
-// fast policy, CUDA's sincosf otherwise.
-template <int SC>
-__device__ __forceinline__ void sincos_angle(float a, float *s, float *c) {
-  if (SC == SC_FAST) __sincosf(a, s, c);
-  else sincosf(a, s, c);
-}
-
 // sin and cos rounded once from a double evaluation: the correctly rounded
 // float result except within ~1e-16 of a rounding midpoint.
 __device__ __forceinline__ float sinf_cr(float x) { return (float)sin((double)x); }
