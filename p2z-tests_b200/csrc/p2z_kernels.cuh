@@ -34,9 +34,11 @@ constexpr int HIT_WORDS = 9;   // 3 pos + 6 cov
 // Kernel kinds
 enum { KIND_FLAT = 0, KIND_PERSISTENT = 1, KIND_STAGED = 2 };
 // Arithmetic of a kernel instance:
-//  UPDK_V2       precise FP32 form, FP64 x/y/phi accumulators, the reference's 2-D update
-//  UPDK_V2_COMP  precise FP32 form with no FP64 at all: float-pair accumulators,
-//                compensated 2x2 determinant
+//  UPDK_V2       precise FP32 form (positions anchored at the last hit, anchored
+//                direction), the reference's 2-D update, compensated 2x2
+//                determinant; no FP64
+//  UPDK_V2_COMP  the same with float-pair accumulators for x and y instead of
+//                anchored positions
 //  UPDK_3X3_F64  precise FP32 propagation; 3x3 inversion + Joseph update in FP64
 //  UPDK_3X3_COMP precise FP32 propagation; 3x3 + Joseph in FP32 with compensated
 //                cofactors, float-pair accumulators (FP64-free)
