@@ -156,19 +156,22 @@ __device__ __forceinline__ void sv_series(float a, float *s, float *v) {
   *v = a2 * pv;
 }
 
-// tan(t + d) from tA = tan(t) and a small offset d (the theta offset, which
-// only sums Kalman corrections of order 1e-3 rad):
-//   tan(t + d) = tA + u (1 + tA^2) / (1 - tA u),  u = tan d = d + d^3/3 + ...,
-// with 1/(1 - x) = 1 + x + x^2 + ... to x^2.  For |d| (1 + |tA|) <= 0.01 the
-// truncations are below 1.4e-11 (u) and 1e-6 of the increment (the quotient,
-// (tA u)^3); the increment is formed first and added to tA last (one rounding
-// at the size of the result).
+// tan(t + d) from tA = tan(t) and an offset d (the theta offset, which sums
+// Kalman corrections: of order 1e-3 rad on well-measured tracks, up to ~0.15
+// rad in one update when the initial angles are off by a few 1e-2):
+//   tan(t + d) = tA + u (1 + tA^2) / (1 - tA u),
+//   u = tan d = d + d^3/3 + 2 d^5/15 + 17 d^7/315 + ...
+// u's series is truncated after d^7 (the next term, 62 d^9/2835, is below
+// 1.2e-8 absolute for |d| <= 0.2); the quotient is exact up to a Newton-refined
+// reciprocal.  The increment is formed first and added to tA last (one
+// rounding at the size of the result).
 __device__ __forceinline__ float tan_offset(float tA, float d) {
-  const float u = fmaf(d * d, d * 0.33333334f, d);
-  const float tu = tA * u;
-  const float q = fmaf(tu, tu, tu);
+  const float d2 = d * d;
+  float p = fmaf(d2, 5.3968254e-2f, 1.3333334e-1f);
+  p = fmaf(d2, p, 3.3333334e-1f);
+  const float u = fmaf(d * d2, p, d);
   const float r = u * fmaf(tA, tA, 1.f);
-  return tA + fmaf(r, q, r);
+  return fmaf(r, rcp_nr(fmaf(-tA, u, 1.f)), tA);
 }
 
 // sin(a) and 1 - cos(a) without cancellation.
@@ -200,10 +203,11 @@ __device__ __forceinline__ void rotated(float c, float s, float w, float v, floa
 // Re-anchoring thresholds of the carried phi and theta offsets.  After a
 // propagation |dP| <= 0.4, so the next step evaluates its phi offset (plus
 // that step's Kalman correction, of order 1e-3 rad) inside the 0.5 rad range
-// of sv_series; |dT| (1 + |tan theta|) <= 0.01 keeps the theta offset inside
-// the range of tan_offset.
+// of sv_series; |dT| <= 0.02 at the start of a propagation keeps the theta
+// offset of the next one (plus one Kalman correction) inside the range of
+// tan_offset.
 constexpr float kAnchorPhi = 0.4f;
-constexpr float kAnchorTheta = 0.01f;
+constexpr float kAnchorTheta = 0.02f;
 
 // ---------------------------------------------------------------------------
 // Track state in registers
@@ -302,7 +306,7 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   }
   h.tanT = tan_offset(s.tT, s.dT);
   h.icT2 = fmaf(h.tanT, h.tanT, 1.f);
-  const bool moveT = fmaf(fabsf(s.tT), fabsf(s.dT), fabsf(s.dT)) > kAnchorTheta;
+  const bool moveT = fabsf(s.dT) > kAnchorTheta;
   s.tT = moveT ? h.tanT : s.tT;
   s.dT = moveT ? 0.f : s.dT;
   h.dzk = (SC == SC_FAST) ? h.deltaZ * ik : __fdiv_rn(h.deltaZ, k);
