@@ -819,8 +819,12 @@ __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float 
   acc_add(s.phi, dphi);
   s.theta = theta_new;
   turn_direction(s, dphi, dth);
-  // Joseph form: P = (I - K H) C, C'' = P - P H^T K^T + K V K^T, with
-  // P(i,j) = C(i,j) - K(i,0) C(0,j) - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0.
+  // Joseph form C'' = (I - K H) C (I - K H)^T + K V K^T, evaluated as
+  // C'' = P - E K^T with P = (I - K H) C and E = P H^T - K V: exact for any
+  // gain, since P (I - K H)^T = P - P H^T K^T.  P(i,j) = C(i,j) - K(i,0) C(0,j)
+  // - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0, so E(i,m) = P(i,m) - (K V)(i,m)
+  // for m = x, y and E(i,z) = -(K V)(i,z).  Three products per element of C''
+  // instead of the five of P - P H^T K^T + K V K^T.
   const U Cm[5][5] = {{C00, C10, C30, C40, C50},
                       {C10, C11, C31, C41, C51},
                       {C30, C31, C33, C43, C53},
@@ -831,20 +835,18 @@ __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float 
   for (int i = 0; i < 5; ++i)
 #pragma unroll
     for (int j = 0; j < 5; ++j) P[i][j] = Cm[i][j] - (K[i][0] * Cm[0][j] + K[i][1] * Cm[1][j]);
-  U KV[5][3];
+  U E[5][3];
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
-    KV[i][0] = K[i][0] * v00 + K[i][1] * v10 + K[i][2] * v20;
-    KV[i][1] = K[i][0] * v10 + K[i][1] * v11 + K[i][2] * v21;
-    KV[i][2] = K[i][0] * v20 + K[i][1] * v21 + K[i][2] * v22;
+    E[i][0] = P[i][0] - (K[i][0] * v00 + K[i][1] * v10 + K[i][2] * v20);
+    E[i][1] = P[i][1] - (K[i][0] * v10 + K[i][1] * v11 + K[i][2] * v21);
+    E[i][2] = -(K[i][0] * v20 + K[i][1] * v21 + K[i][2] * v22);
   }
   U N[5][5];
 #pragma unroll
   for (int i = 0; i < 5; ++i)
 #pragma unroll
-    for (int j = 0; j <= i; ++j)
-      N[i][j] = P[i][j] - (P[i][0] * K[j][0] + P[i][1] * K[j][1]) +
-                (KV[i][0] * K[j][0] + KV[i][1] * K[j][1] + KV[i][2] * K[j][2]);
+    for (int j = 0; j <= i; ++j) N[i][j] = P[i][j] - (E[i][0] * K[j][0] + E[i][1] * K[j][1] + E[i][2] * K[j][2]);
   s.c00 = float(N[0][0]); s.c10 = float(N[1][0]); s.c11 = float(N[1][1]);
   s.c30 = float(N[2][0]); s.c31 = float(N[2][1]); s.c33 = float(N[2][2]);
   s.c40 = float(N[3][0]); s.c41 = float(N[3][1]); s.c43 = float(N[3][2]); s.c44 = float(N[3][3]);
