@@ -330,6 +330,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample_events_per_step": n_ev, "host_threads": cores},
             "cpu_baseline": {"value": value, "unit": "updates/s", "cores": cores, "kind": "reference",
+                             "cpu_model": cpu_model(),
                              "sample": f"{n_ev} events x 9600 tracks x 20 layers per step, OpenMP over events"},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -339,6 +340,18 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+
+def cpu_model():
+    """The host CPU's model name (as lscpu reports it), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
 
 def cpu_baseline(p2z, trk, hit):
     """The reference's hot loop on this host's cores, on a bounded sample."""
@@ -358,6 +371,7 @@ def cpu_baseline(p2z, trk, hit):
         sec += time.perf_counter() - t0
         reps += 1
     return {"value": n_ev * 9600 * 20 * reps / sec, "unit": "updates/s", "cores": cores, "kind": "reference",
+            "cpu_model": cpu_model(),
             "sample": f"{n_ev} of the 1000 events, {reps} passes ({sec:.1f} s wall), reference OMP build, "
                       f"{cores} threads"}
 
