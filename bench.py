@@ -217,6 +217,28 @@ def barrier(world):
         dist.barrier()
 
 
+def order_by_hits(torch, counts, udt, udh, udm):
+    """Copies of an uneven sample with each event's tracks in order of their hit
+    count (most hits first, padding slots last) and the slot permutation.  A
+    32-track batch runs as one warp, which takes as many steps as its longest
+    track, so batches of similar-length tracks keep every lane busy; callers
+    get this by ordering tracks when they pack an event's batches."""
+    nslots = udm.numel()
+    nb, nlayer = udh.shape[0], udh.shape[1]
+    m = udm.to(torch.int64) & 0xFFFFFFFF
+    pc = torch.zeros(nslots, dtype=torch.int64, device=udm.device)
+    for b in range(32):
+        pc += (m >> b) & 1
+    per_event = torch.as_tensor(((counts + 31) // 32) * 32, device=udm.device)
+    ev = torch.repeat_interleave(torch.arange(len(counts), device=udm.device), per_event)
+    perm = torch.sort(ev * 64 + (32 - pc), stable=True).indices
+    ts = udt.permute(0, 2, 1).reshape(nslots, -1)[perm].reshape(nb, 32, -1).permute(0, 2, 1).contiguous()
+    hs = udh.permute(0, 3, 1, 2).reshape(nslots, nlayer, -1)[perm]
+    hs = hs.reshape(nb, 32, nlayer, -1).permute(0, 2, 3, 1).contiguous()
+    util = lambda x: float(x.sum()) / float(32 * x.reshape(-1, 32).max(1).values.sum())
+    return ts, hs, udm[perm].contiguous(), perm, util(pc), util(pc[perm])
+
+
 def uneven_counts(n_events, seed):
     rng = np.random.default_rng(seed)
     c = np.exp(np.log(3000.0) + 1.0 * rng.standard_normal(n_events))
@@ -521,31 +543,55 @@ def main():
                 r = min((r for r in rows if r["bsize"] == 32 and r["layout"] == "aosoa" and r["schedule"] == sched),
                         key=lambda r: r["ms"])
                 blocks[sched] = r["block_threads"]
-        for sched in ("persistent", "per_event"):
-            c = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=sched,
-                                block_threads=blocks[sched])
+        def timed(c, t, h, mk, o):
+            """updates/s of c on (t, h, mk) -> o, CUDA events on our stream, max over ranks"""
+            run_args = (ctx.h, p2z.C.byref(c), t.data_ptr(), h.data_ptr(), mk.data_ptr(), o.data_ptr(),
+                        p2z.C.c_void_p(stream.cuda_stream), None)
             for _ in range(3):
-                p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), udt.data_ptr(), udh.data_ptr(), udm.data_ptr(),
-                                       udo.data_ptr(), p2z.C.c_void_p(stream.cuda_stream), None)
+                p2z.lib.p2z_run_device(*run_args)
             torch.cuda.synchronize()
             barrier(world)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             n = max(3, args.steps // 2)
             a.record(stream)
             for _ in range(n):
-                p2z.lib.p2z_run_device(ctx.h, p2z.C.byref(c), udt.data_ptr(), udh.data_ptr(), udm.data_ptr(),
-                                       udo.data_ptr(), p2z.C.c_void_p(stream.cuda_stream), None)
+                p2z.lib.p2z_run_device(*run_args)
             b.record(stream)
             torch.cuda.synchronize()
             t_ms = barrier_max(world, a.elapsed_time(b)) / n
-            res[sched] = u_upd * world / (t_ms / 1e3)
+            return u_upd * world / (t_ms / 1e3)
+
+        def cfg_for(sched):
+            return p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=sched,
+                                   block_threads=blocks.get(sched, 32))
+
+        for sched in ("persistent", "per_event"):
+            res[sched] = timed(cfg_for(sched), udt, udh, udm, udo)
+        # the same sample with each event's tracks ordered by hit count (a packing choice of the caller)
+        ts, hs, ms_, perm, util_packed, util_ordered = order_by_hits(torch, counts, udt, udh, udm)
+        ordered = {}
+        for sched in ("persistent", "flat"):
+            ordered[sched] = timed(cfg_for(sched), ts, hs, ms_, udo)
+        # same per-track results: the ordered run's outputs, put back in packed order, equal the packed run's
+        uo = torch.empty_like(udo)
+        ctx.run_device(cfg_for("persistent"), udt, udh, udo, d_mask=udm)
+        ctx.run_device(cfg_for("persistent"), ts, hs, uo, d_mask=ms_)
+        back = torch.empty_like(uo.permute(0, 2, 1).reshape(perm.numel(), -1))
+        back[perm] = uo.permute(0, 2, 1).reshape(perm.numel(), -1)
+        same = bool((back.view(torch.int32) == udo.permute(0, 2, 1).reshape(perm.numel(), -1).view(torch.int32)).all())
         bvp = {"workload": "2000 events, track counts log-normal (median 3000, sigma 1, clipped 50-30000), "
                            "5-20 hits/track, 10% layers dropped",
                "tracks": int(counts.sum()), "updates_per_step": u_upd,
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
                "ratio": res["persistent"] / res["per_event"], "block_threads": blocks,
+               "ordered_by_hits": {"note": "same events, each event's tracks packed in order of hit count",
+                                   "batched_persistent_graph": ordered["persistent"],
+                                   "flat": ordered["flat"], "ratio_vs_plain": ordered["persistent"] / res["per_event"],
+                                   "lane_utilisation_as_packed": util_packed,
+                                   "lane_utilisation_ordered": util_ordered,
+                                   "same_results_as_packed": same},
                "autotune": tune_uneven}
-        del udt, udh, udo, udm
+        del udt, udh, udo, udm, ts, hs, ms_, uo, back
 
     # serving: continuous batching under Poisson arrivals
     serving = None
