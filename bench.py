@@ -569,6 +569,7 @@ def main():
             res[sched] = timed(cfg_for(sched), udt, udh, udm, udo)
         # the same sample with each event's tracks ordered by hit count (a packing choice of the caller)
         ts, hs, ms_, perm, util_packed, util_ordered = order_by_hits(torch, counts, udt, udh, udm)
+        torch.cuda.synchronize()  # the copies are made on torch's stream; the runs read them on ours
         ordered = {}
         for sched in ("persistent", "flat"):
             ordered[sched] = timed(cfg_for(sched), ts, hs, ms_, udo)
