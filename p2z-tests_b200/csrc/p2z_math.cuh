@@ -8,9 +8,10 @@
 //
 // Two evaluation forms of that algebra are provided:
 //
-// FORM_PRECISE (the default): FP32 bulk arithmetic, evaluated so that it agrees
-//   with an all-FP64 evaluation to ~1e-6 in the parameters.  Two changes from
-//   the reference's FP32 evaluation, both exact in real arithmetic:
+// FORM_PRECISE (the default): FP32 arithmetic, no FP64 instruction, evaluated
+//   so that it agrees with an all-FP64 evaluation to a few 1e-6 in the
+//   parameters.  Three changes from the reference's FP32 evaluation, all exact
+//   in real arithmetic:
 //   * 1 - cos(a), for the helix angle a = alpha and for a = cosP*sin(alpha),
 //     is computed as the versine directly (a Taylor series of
 //     a^2/2 - a^4/24 + ..., or 2 sin^2(a/2)) instead of subtracting a rounded
@@ -22,6 +23,9 @@
 //     exact, plus an FP32 offset) -- or as float pairs, or in FP64 for the
 //     all-FP64 kernel: positions of tens of cm held in FP32 round at ~4e-6 cm,
 //     which against 30 um hits biases the curvature.
+//   * the direction (cos/sin phi, tan theta) is an anchor advanced once per
+//     step by the angle increments summed since the anchor, instead of sin/cos
+//     of rounded accumulated angles (see Trk and propagate_params_precise).
 // FORM_REFERENCE: the reference's FP32 evaluation operation for operation,
 //   including its C type promotions (the double literals in `1./ipt`,
 //   `1.0/cosT`, `(1.-cosa)` ... and the double determinant), for callers who
