@@ -324,6 +324,48 @@ def num_batches(cfg: Config) -> int:
     return n
 
 
+# cudaStreamLegacy: the legacy default stream, which the C API takes only as
+# this explicit handle (a NULL stream means the context's own stream).
+CUDA_STREAM_LEGACY = 0x1
+
+
+def _torch_cuda(arrays):
+    """The first torch CUDA tensor among arrays, or None."""
+    for a in arrays:
+        if a is not None and type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False):
+            return a
+    return None
+
+
+def _stream(stream, *arrays):
+    """The stream handle a device call runs on.  An explicit stream (a handle
+    or an object with .cuda_stream) is used as given.  Without one, a call on
+    torch CUDA tensors runs on torch's current stream of their device: the
+    library's kernels then follow the torch work that wrote those tensors, and
+    no pending torch work can still be reading memory that torch's allocator
+    has handed out again as one of them (the library's own stream is not
+    ordered with torch's).  Otherwise None: the context's stream."""
+    if stream is not None:
+        h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        return h if h != 0 else CUDA_STREAM_LEGACY
+    t = _torch_cuda(arrays)
+    if t is None:
+        return None
+    import torch
+    h = torch.cuda.current_stream(t.device).cuda_stream
+    return h if h != 0 else CUDA_STREAM_LEGACY
+
+
+def _wait_for_torch(*arrays):
+    """Before a call that runs on the context's stream only: wait for torch's
+    current stream when torch CUDA tensors are among the arguments (the same
+    ordering _stream gives the calls that take a stream)."""
+    t = _torch_cuda(arrays)
+    if t is not None:
+        import torch
+        torch.cuda.current_stream(t.device).synchronize()
+
+
 def _ptr(a) -> int | None:
     if a is None:
         return None
@@ -491,22 +533,26 @@ class Context:
     def run_device(self, cfg: Config, d_trk_in, d_hits, d_trk_out, d_mask=None, stream=None, stats=True):
         """Device-memory pass; pointers are ints or objects with data_ptr()."""
         st = Stats() if stats else None
+        stream = _stream(stream, d_trk_in, d_hits, d_mask, d_trk_out)
         _check(lib.p2z_run_device(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits), _ptr(d_mask),
                                   _ptr(d_trk_out), stream, C.byref(st) if st is not None else None), self.h)
         return st
 
     def step_device(self, bsize, nbatches, d_trk, d_hits, nlayer, layer, what=3, update=UPDATE_V2, kfact=0.0):
+        _wait_for_torch(d_trk, d_hits)
         _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
                                    kfact), self.h)
 
     def generate_physics_device(self, cfg: Config, d_trk, d_hits, d_mask=None, params=None, stream=None):
         """The physics sample generated on the device (p2z_generate_physics_device)."""
         params = params or physics_params()
+        stream = _stream(stream, d_trk, d_hits, d_mask)
         _check(lib.p2z_generate_physics_device(self.h, C.byref(params), C.byref(cfg), _ptr(d_trk), _ptr(d_hits),
                                                _ptr(d_mask), stream), self.h)
 
     def mask_layers_device(self, d_mask, nslots, nlayer, min_hits=5, max_hits=20, drop_prob=0.1, seed=7,
                            stream=None):
+        stream = _stream(stream, d_mask)
         _check(lib.p2z_mask_layers_device(self.h, _ptr(d_mask), nslots, nlayer, min_hits, max_hits, drop_prob,
                                           seed, stream), self.h)
 
@@ -514,6 +560,7 @@ class Context:
         """The validation block reduced on the GPU (p2z_validate_device)."""
         h = (C.c_float * 3)(*hit_last)
         v = Validation()
+        stream = _stream(stream, d_trk_out)
         _check(lib.p2z_validate_device(self.h, _ptr(d_trk_out), bsize, nevts, ntrks, h, C.byref(v), stream), self.h)
         return v
 
@@ -521,6 +568,7 @@ class Context:
         h = (C.c_float * 3)(*hit_last)
         m = None if means is None else (C.c_double * 6)(*means)
         acc = ValidationPartial()
+        stream = _stream(stream, d_trk_out)
         _check(lib.p2z_validate_partial_device(self.h, _ptr(d_trk_out), bsize, nevts, ntrks, h, m, C.byref(acc),
                                                stream), self.h)
         return acc
@@ -528,6 +576,7 @@ class Context:
     def relayout_device(self, cfg_from: Config, cfg_to: Config, d_trk_in, d_hits_in, d_trk_out, d_hits_out,
                         d_mask_in=None, d_mask_out=None, stream=None):
         """Convert device arrays between bsizes / AOSOA / SoA (p2z_relayout_device)."""
+        stream = _stream(stream, d_trk_in, d_hits_in, d_mask_in, d_trk_out, d_hits_out, d_mask_out)
         _check(lib.p2z_relayout_device(self.h, C.byref(cfg_from), C.byref(cfg_to), _ptr(d_trk_in), _ptr(d_hits_in),
                                        _ptr(d_mask_in), _ptr(d_trk_out), _ptr(d_hits_out), _ptr(d_mask_out),
                                        stream), self.h)
@@ -538,6 +587,7 @@ class Context:
         rows = (TuneEntry * max_entries)()
         n = C.c_int(0)
         best = TuneEntry()
+        _wait_for_torch(d_trk_in, d_hits, d_mask)
         _check(lib.p2z_autotune(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits), _ptr(d_mask), reps, rows,
                                 max_entries, C.byref(n), C.byref(best)), self.h)
         entries = sorted((rows[i].as_dict() for i in range(min(n.value, max_entries))), key=lambda d: d["ms"])

@@ -306,11 +306,15 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
       ctx->gexec = nullptr;
     }
     ctx->has_graph = false;
+    // The graph is recorded on the context's own stream, which can always be
+    // captured (the caller's may be the legacy default stream, which cannot),
+    // and replayed on the caller's stream below.
     cudaGraph_t g = nullptr;
-    P2Z_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
-    cudaError_t e2 = dispatch(spec, st);
-    cudaError_t e3 = cudaStreamEndCapture(st, &g);
+    cudaStream_t cs = ctx->stream;
+    P2Z_CUDA(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), cs);
+    cudaError_t e2 = dispatch(spec, cs);
+    cudaError_t e3 = cudaStreamEndCapture(cs, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
