@@ -334,7 +334,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference tree)"}))
         return 0
     cores = os.cpu_count() or 1
-    n_ev = args.ref_events
+    n_ev = args.ref_events or cpu_sample_events(cores)
     cfg = p2z.make_config(bsize=32, nevts=n_ev, ntrks=9600, nlayer=20)
     trk, hit = p2z.generate_physics(cfg)
     upd = n_ev * 9600 * 20
@@ -375,6 +375,13 @@ def cpu_model():
     return None
 
 
+def cpu_sample_events(cores):
+    """Events in a CPU sample: a multiple of the thread count near 64, since
+    the reference spreads whole events over its OpenMP threads (50 events on
+    16 threads would leave the busiest thread 4 against an average of 3.1)."""
+    return cores * max(1, round(64 / cores))
+
+
 def cpu_baseline(p2z, trk, hit):
     """The reference's hot loop on this host's cores, on a bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -382,7 +389,7 @@ def cpu_baseline(p2z, trk, hit):
     if not O.ref_available("b32"):
         return None
     cores = os.cpu_count() or 1
-    n_ev = 50
+    n_ev = cpu_sample_events(cores)
     nb = n_ev * 300
     t, h = np.ascontiguousarray(trk[:nb]), np.ascontiguousarray(hit[:nb])
     O.ref_run(t, h, nev=n_ev, nthreads=cores)
@@ -404,7 +411,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-events", type=int, default=50)
+    ap.add_argument("--ref-events", type=int, default=0,
+                    help="events per reference step (0: a multiple of the thread count near 64)")
     ap.add_argument("--nevts", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
@@ -447,7 +455,7 @@ def main():
     updates = nev * 9600 * 20
     do = torch.empty_like(dt)
     # host copy of the first events for the CPU baseline (rank 0)
-    n_cpu_ev = 50
+    n_cpu_ev = cpu_sample_events(os.cpu_count() or 1)
     cpu_sample = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_sample = (dt[:n_cpu_ev * 300].cpu().numpy(), dh[:n_cpu_ev * 300].cpu().numpy())
