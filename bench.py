@@ -49,6 +49,11 @@ ROOT = pathlib.Path(__file__).resolve().parent
 #   Compulsory bytes: 6 hit words (24 B) + track in and out (2 x 112 B) over
 #   20 layers (11.2 B) = 35.2 B.
 FLOPS_PER_UPDATE = 349
+# The same update counted as the reference writes it (its propagateToZ
+# scalars, the full MultHelixPropEndcap / MultHelixPropTranspEndcap products
+# including those with J's known zeros, KalmanUpdate_v2): ~460 FP32 flops.
+# Reported beside the reduced count, never in place of it.
+FLOPS_PER_UPDATE_REFERENCE_FORM = 460
 BYTES_PER_UPDATE = 35.2
 FP32_LANES_PER_SM = 128
 
@@ -640,7 +645,12 @@ def main():
         "fp32_roofline": {"achieved": fp32_ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": fp32_ach / fp32_peak,
                           "flops_per_update": FLOPS_PER_UPDATE,
                           "peak_source": f"148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (nominal, no measured "
-                                         f"FP32 peak on this pool)"},
+                                         f"FP32 peak on this pool)",
+                          "reference_form": {
+                              "flops_per_update": FLOPS_PER_UPDATE_REFERENCE_FORM,
+                              "frac": FLOPS_PER_UPDATE_REFERENCE_FORM * updates / (launch_ms / 1e3) / 1e12 / fp32_peak,
+                              "note": "the update counted as the reference writes it, products with the "
+                                      "Jacobian's known zeros included; this kernel does not execute those"}},
         "clocks": clk,
         "autotune": tune_head,
         "gpu_launches": launches_per_step * args.steps,
