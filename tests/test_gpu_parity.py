@@ -417,6 +417,34 @@ def test_full_size_properties(p2z, oracle, ctx):
     assert par_rel(gs["par"], o64[:, :6]).max() <= PREC_PAR
 
 
+def test_arrays_beyond_2_31_words(p2z, ctx):
+    """Index arithmetic past 2^31 words: 4000 events x 9600 tracks put 6.9e9
+    words in the hit array (27.6 GB) and 1.1e9 in each track array.  The
+    generator fills a slot from (seed, global slot index) alone, so batches
+    beyond the 2^31-word mark, copied out and run on their own, must give the
+    bits the full-size run gave them."""
+    import torch
+    cfg = p2z.make_config(bsize=32, nevts=4000, ntrks=9600, nlayer=20)
+    nb = p2z.num_batches(cfg)
+    hit_words_per_batch = 20 * 9 * 32
+    assert nb * hit_words_per_batch > 3 * 2 ** 31
+    dt = torch.empty((nb, 28, 32), device="cuda")
+    dh = torch.empty((nb, 20, 9, 32), device="cuda")
+    ctx.generate_physics_device(cfg, dt, dh)
+    do = torch.empty_like(dt)
+    st = ctx.run_device(cfg, dt, dh, do)
+    assert st.updates == 4000 * 9600 * 20 and st.singular == 0
+    one = p2z.make_config(bsize=32, nevts=1, ntrks=32, nlayer=20)
+    for b in (2 ** 31 // hit_words_per_batch + 1, 2 ** 32 // hit_words_per_batch + 3, nb - 1):
+        t, h = dt[b:b + 1].cpu().numpy(), dh[b:b + 1].cpu().numpy()
+        alone = np.empty_like(t)
+        ctx.run(one, t, h, alone)
+        assert _bitdiff(alone, do[b:b + 1].cpu().numpy()) == 0, b
+    assert bool(torch.isfinite(do[:, :27, :]).all())
+    del dt, dh, do
+    torch.cuda.empty_cache()
+
+
 PREC_PAR_FULL = 5e-6
 
 
