@@ -211,8 +211,13 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
                    const uint32_t *hit_mask, void *trk_out, p2z_stats *stats);
 
 /* Same pass on DEVICE-resident buffers, enqueued on `stream` (a cudaStream_t;
- * NULL = the context's stream).  Returns after enqueueing (asynchronous) unless
- * stats != NULL, in which case it synchronises to fill the timings.
+ * NULL = the context's stream, cudaStreamLegacy = the legacy default stream).
+ * The context's stream is not ordered with any other: a caller whose buffers
+ * come from work on another stream passes that stream, or synchronises it
+ * first.  Returns after enqueueing (asynchronous) unless stats != NULL, in
+ * which case it synchronises to fill the timings.  The PERSISTENT schedule's
+ * graph is recorded on the context's stream and replayed on `stream`; while
+ * `stream` is itself being captured, the kernels are launched into it directly.
  * d_trk_out must not alias d_trk_in.  Replaces GPUsequence/GPUsequenceR
  * (src/propagate-toz-test_CUDA_v4.cu:746-828). */
 p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
