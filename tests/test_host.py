@@ -197,3 +197,20 @@ def test_dump_tracks_writes_the_selected_tracks(p2z, tmp_path):
     for name, row in (("input_x.txt", 0), ("input_y.txt", 1), ("input_z.txt", 2)):
         assert (tmp_path / name).read_text().split() == ["%f" % v for v in trk_in[0, row, kept].astype(np.float64)]
     assert len((tmp_path / "output_z.txt").read_text().split()) == len(kept)
+
+
+def test_device_call_stream_selection(p2z):
+    """The binding's choice of stream for a device call: an explicit stream
+    (handle or object with .cuda_stream) as given, the legacy default stream's
+    handle 0 as cudaStreamLegacy (NULL means the context's own stream in the
+    C ABI), and no stream for arguments that are not torch CUDA tensors."""
+    class FakeStream:
+        def __init__(self, h):
+            self.cuda_stream = h
+    assert p2z._stream(0) == p2z.CUDA_STREAM_LEGACY
+    assert p2z._stream(0x7f00) == 0x7f00
+    assert p2z._stream(FakeStream(0)) == p2z.CUDA_STREAM_LEGACY
+    assert p2z._stream(FakeStream(0x5000)) == 0x5000
+    assert p2z._stream(None, np.zeros(4, np.float32), 12345, None) is None
+    import torch
+    assert p2z._stream(None, torch.zeros(4)) is None  # a CPU tensor
