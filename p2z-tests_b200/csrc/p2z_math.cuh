@@ -76,7 +76,6 @@ __device__ __forceinline__ float tof(float v) { return v; }
 __device__ __forceinline__ float tof(AP v) { return v.a + v.u; }
 __device__ __forceinline__ float tof(double v) { return (float)v; }
 __device__ __forceinline__ float tof(DF v) { return v.hi + v.lo; }
-__device__ __forceinline__ double tod(double v) { return v; }
 
 __device__ __forceinline__ void acc_set(float &a, float v) { a = v; }
 __device__ __forceinline__ void acc_set(double &a, float v) { a = v; }
