@@ -58,7 +58,7 @@ BYTES_PER_UPDATE = 35.2
 FP32_LANES_PER_SM = 128
 
 METRIC = "track-layer updates/s on 1 B200, batched vs plain, <=1e-5 rel err vs FP64"
-WORKLOAD = "physics 1000 events x 9600 tracks x 20 layers, bsize 32, FP32 (precise form)"
+WORKLOAD = "physics 1000 events x 9600 tracks x 20 layers, bsize 32, FP32"
 
 
 def load_p2z():
@@ -327,12 +327,22 @@ def run_serving(p2z, device, rank, args):
 # reference arm
 # ---------------------------------------------------------------------------
 
+def workload_config(nev, world):
+    """The workload's description, identical in both arms."""
+    return {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
+            "updates_per_step_per_gpu": nev * 9600 * 20, "l2": "inputs 8.1 GB > L2, no flush",
+            "parallelism": f"dp{world} (independent event shards)"}
+
+
 def run_reference(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    """The reference's own OpenMP hot loop (src/propagate-toz-test_OMP.cpp
+    compiled unchanged into oracle/_ref) on this host's cores.  Its inputs are
+    the same physics sample, generated by the oracle's restatement of the
+    generator: nothing of the product library is loaded in this arm."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    p2z = load_p2z()
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     if not O.ref_available("b32"):
@@ -340,8 +350,7 @@ def run_reference(args):
         return 0
     cores = os.cpu_count() or 1
     n_ev = args.ref_events or cpu_sample_events(cores)
-    cfg = p2z.make_config(bsize=32, nevts=n_ev, ntrks=9600, nlayer=20)
-    trk, hit = p2z.generate_physics(cfg)
+    trk, hit = O.physics(32, n_ev, 9600, 20, seed=20240601)
     upd = n_ev * 9600 * 20
     for _ in range(args.warmup):
         O.ref_run(trk, hit, nev=n_ev, nthreads=cores)
@@ -352,13 +361,16 @@ def run_reference(args):
         ts.append(time.perf_counter() - t0)
     sec = float(np.sum(ts))
     value = upd * args.steps / sec
+    sample = (f"{n_ev} of the {args.nevts} events x 9600 tracks x 20 layers per step "
+              f"({upd} updates), OpenMP over events, {cores} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_events_per_step": n_ev, "host_threads": cores},
+            "config": workload_config(args.nevts, world),
+            "sample": {"events_per_step": n_ev, "updates_per_step": upd, "host_threads": cores,
+                       "inputs": "the physics sample (seed 20240601) from the oracle's generator"},
             "cpu_baseline": {"value": value, "unit": "updates/s", "cores": cores, "kind": "reference",
-                             "cpu_model": cpu_model(),
-                             "sample": f"{n_ev} events x 9600 tracks x 20 layers per step, OpenMP over events"},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -629,14 +641,12 @@ def main():
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
-                   "updates_per_step_per_gpu": updates, "l2": "inputs 8.1 GB > L2, no flush",
-                   "parallelism": f"dp{world} (independent event shards)",
-                   "launch": {"schedule": (args.schedule if args.schedule != "auto" else
-                                           (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
-                              "block_threads": (args.block or
-                                                (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head
-                                                 else 128))}},
+        "config": workload_config(nev, world),
+        "form": "precise (default; no FP64 instruction)",
+        "launch": {"schedule": (args.schedule if args.schedule != "auto" else
+                                (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
+                   "block_threads": (args.block or
+                                     (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head else 128))},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": (tpu * updates / launches_per_step) if tpu else None,

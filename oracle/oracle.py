@@ -9,6 +9,10 @@ legs import this module.  It loads:
 * ``_ref/<isa>/libp2zref_*.so`` -- the reference benchmark's own OpenMP source
   (src/propagate-toz-test_OMP.cpp) compiled unchanged by oracle/Makefile.
 
+``physics()`` generates the benchmark's physics sample from the restatement
+in p2z_physics_oracle.c (part of liboracle.so), so that the benchmark's
+reference arm builds its inputs without the product library.
+
 Both are built by ``make -C oracle oracle ref`` (the ``ref`` target needs the
 reference tree; its outputs travel with the repository snapshot).
 """
@@ -67,6 +71,38 @@ def oracle_lib(cr_trig: bool = False):
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+class PhysicsParams(C.Structure):
+    """The physics sample's parameters (field order of the library's
+    p2z_physics_params; defaults: the benchmark's physics workload)."""
+    _fields_ = [("seed", C.c_uint64), ("pt_min", C.c_double), ("pt_max", C.c_double), ("eta_min", C.c_double),
+                ("eta_max", C.c_double), ("sigma_vz", C.c_double), ("sig_xy", C.c_double), ("sig_z", C.c_double),
+                ("rel_sig_ipt", C.c_double), ("sig_phi", C.c_double), ("sig_theta", C.c_double),
+                ("rho_max", C.c_double), ("z_first", C.c_double), ("z_last", C.c_double),
+                ("hit_sig_xy", C.c_double), ("hit_sig_z", C.c_double), ("kfact", C.c_float),
+                ("nthreads", C.c_int32)]
+
+    DEFAULTS = dict(seed=20240601, pt_min=0.5, pt_max=20.0, eta_min=1.6, eta_max=2.5, sigma_vz=5.0, sig_xy=0.01,
+                    sig_z=0.05, rel_sig_ipt=0.01, sig_phi=1e-3, sig_theta=1e-3, rho_max=0.3, z_first=30.0,
+                    z_last=270.0, hit_sig_xy=30e-4, hit_sig_z=1e-4, kfact=0.0, nthreads=0)
+
+    def __init__(self, **kw):
+        super().__init__(**{**self.DEFAULTS, **kw})
+
+
+def physics(bsize: int, nevts: int, ntrks: int, nlayer: int = 20, **params):
+    """The physics sample (uniform events) as (trk (nb,28,B), hits (nb,nl,9,B)) float32."""
+    lib = oracle_lib()
+    lib.oph_generate.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_void_p, C.c_void_p]
+    lib.oph_generate.restype = C.c_int
+    nb = nevts * ntrks // bsize
+    trk = np.empty((nb, 28, bsize), dtype=np.float32)
+    hit = np.empty((nb, nlayer, 9, bsize), dtype=np.float32)
+    prm = PhysicsParams(**params)
+    if lib.oph_generate(C.byref(prm), bsize, nevts, ntrks, nlayer, _p(trk), _p(hit)):
+        raise ValueError("bad physics sample size")
+    return trk, hit
 
 
 def kfact_default() -> float:
