@@ -55,6 +55,8 @@ FLOPS_PER_UPDATE = 349
 # Reported beside the reduced count, never in place of it.
 FLOPS_PER_UPDATE_REFERENCE_FORM = 460
 BYTES_PER_UPDATE = 35.2
+BYTES_HIT_PER_UPDATE = 24   # the 6 hit words a 2-D update reads
+BYTES_TRACK = 228           # a track read and written (2 x 112 B) and its mask word
 FP32_LANES_PER_SM = 128
 
 METRIC = "track-layer updates/s on 1 B200, batched vs plain, <=1e-5 rel err vs FP64"
@@ -242,6 +244,20 @@ def order_by_hits(torch, counts, udt, udh, udm):
     hs = hs.reshape(nb, 32, nlayer, -1).permute(0, 2, 3, 1).contiguous()
     util = lambda x: float(x.sum()) / float(32 * x.reshape(-1, 32).max(1).values.sum())
     return ts, hs, udm[perm].contiguous(), perm, util(pc), util(pc[perm])
+
+
+def window_util(mask, win):
+    """Lane utilisation of a masked run whose 256-slot windows are processed
+    in order of hit count: present-hit lane-steps over 32 x the warps' steps."""
+    import torch
+    m = mask.to(torch.int64) & 0xFFFFFFFF
+    pc = torch.zeros_like(m)
+    for b in range(32):
+        pc += (m >> b) & 1
+    n = (pc.numel() + win - 1) // win * win
+    pc = torch.nn.functional.pad(pc, (0, n - pc.numel()))
+    s = torch.sort(pc.view(-1, win), dim=1, descending=True).values
+    return float(pc.sum()) / float(32 * s.view(-1, 32).max(1).values.sum())
 
 
 def uneven_counts(n_events, seed):
@@ -456,6 +472,9 @@ def main():
     # A stream of our own: its handle is never the legacy default stream (0),
     # which the C ABI would read as "the context's stream".
     stream = torch.cuda.Stream()
+    # measured denominators on this GPU and its host link, before any timing
+    live_peaks = p2z.measure_peaks(local)
+    fp32_peak_live = max(live_peaks["fp32_ffma_tflops"], live_peaks["fp32_ffma2_tflops"])
 
     nev = args.nevts
     # schedule and block size left open: the context applies what p2z_autotune measured
@@ -534,10 +553,20 @@ def main():
             s = ctx.run(ecfg, pin_t.array, pin_h.array, pin_o.array)
             tot += s.total_ms
         tot = barrier_max(world, tot)
-        e2e = {"value": updates * world / (tot / n_e2e / 1e3), "unit": "updates/s",
+        e2e_ms = tot / n_e2e
+        # the host link's floor for this step: each direction at its measured
+        # pinned rate, and both together at the measured two-way rate
+        link_ms = 1e3 * max(s.h2d_bytes / (live_peaks["h2d_gbs"] * 1e9), s.d2h_bytes / (live_peaks["d2h_gbs"] * 1e9),
+                            (s.h2d_bytes + s.d2h_bytes) / (live_peaks["bidir_gbs"] * 1e9))
+        e2e = {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s",
                "h2d_bytes_per_step": int(s.h2d_bytes), "d2h_bytes_per_step": int(s.d2h_bytes),
-               "ms_per_step": tot / n_e2e, "steps": n_e2e,
-               "path": "p2z_run, pinned host buffers, 8 chunks on 2 streams (copy/compute overlap)"}
+               "ms_per_step": e2e_ms, "steps": n_e2e,
+               "path": "p2z_run, pinned host buffers, 8 chunks on 2 streams (copy/compute overlap)",
+               "roofline": {"bound": "host link (PCIe)", "link_floor_ms": link_ms, "frac": link_ms / e2e_ms,
+                            "ceiling_updates_per_s": updates * world / (link_ms / 1e3),
+                            "peaks": {k: live_peaks[k] for k in ("h2d_gbs", "d2h_gbs", "bidir_gbs")},
+                            "peak_source": "measured in this run: p2z_measure_peaks, one 1 GiB pinned "
+                                           "cudaMemcpyAsync each way and both at once, best of 5"}}
         out_ok = bool(np.isfinite(pin_o.array[:, :6, :]).all())
         pin_t.free(); pin_h.free(); pin_o.free()
     else:
@@ -592,6 +621,14 @@ def main():
 
         for sched in ("persistent", "per_event"):
             res[sched] = timed(cfg_for(sched), udt, udh, udm, udo)
+        # the same batched run with each 256-slot window in order of hit count (in-library sort)
+        csw = cfg_for("persistent")
+        csw.flags |= p2z.FLAG_SORT_WINDOWS
+        res["persistent_sorted_windows"] = timed(csw, udt, udh, udm, udo)
+        # the plain form as the reference's GPU build issues it: launches spread over 10 streams
+        c10 = cfg_for("per_event")
+        c10.flags |= p2z.FLAG_PER_EVENT_STREAMS
+        res["per_event_10_streams"] = timed(c10, udt, udh, udm, udo)
         # the same sample with each event's tracks ordered by hit count (a packing choice of the caller)
         ts, hs, ms_, perm, util_packed, util_ordered = order_by_hits(torch, counts, udt, udh, udm)
         torch.cuda.synchronize()  # the copies are made on torch's stream; the runs read them on ours
@@ -609,7 +646,23 @@ def main():
                            "5-20 hits/track, 10% layers dropped",
                "tracks": int(counts.sum()), "updates_per_step": u_upd,
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
-               "ratio": res["persistent"] / res["per_event"], "block_threads": blocks,
+               "plain_per_event_launch_10_streams": res["per_event_10_streams"],
+               "batched_persistent_graph_sorted_windows": res["persistent_sorted_windows"],
+               "lane_utilisation": {"stored_order": util_packed, "sorted_windows": window_util(udm, 256),
+                                    "note": "present-hit lane-steps / (32 x warp steps); sorted_windows: each "
+                                            "256-slot window in order of hit count (P2Z_FLAG_SORT_WINDOWS)"},
+               "ratio": res["persistent"] / res["per_event"],
+               "ratio_vs_10_streams": res["persistent"] / res["per_event_10_streams"],
+               "batched_roofline": {
+                   "fp32_tflops": FLOPS_PER_UPDATE * res["persistent"] / 1e12,
+                   "fp32_frac": FLOPS_PER_UPDATE * res["persistent"] / 1e12 / fp32_peak_live,
+                   "hbm_gbs": (BYTES_HIT_PER_UPDATE * res["persistent"] +
+                               BYTES_TRACK * int(counts.sum()) * res["persistent"] / u_upd) / 1e9,
+                   "hbm_frac": (BYTES_HIT_PER_UPDATE * res["persistent"] +
+                                BYTES_TRACK * int(counts.sum()) * res["persistent"] / u_upd) / 1e9 /
+                               measured_peaks()["hbm_gbs"],
+                   "note": "present-hit updates; bytes = 24 per present hit + 228 per real track (in, out, mask)"},
+               "block_threads": blocks,
                "ordered_by_hits": {"note": "same events, each event's tracks packed in order of hit count",
                                    "batched_persistent_graph": ordered["persistent"],
                                    "flat": ordered["flat"], "ratio_vs_plain": ordered["persistent"] / res["per_event"],
@@ -635,7 +688,8 @@ def main():
     achieved_gbs = BYTES_PER_UPDATE * updates / launches_per_step / (launch_ms / 1e3) / 1e9
     tpu = profile_traffic_per_update()
     sm_max = clk["sm_max_mhz"] or 1965.0
-    fp32_peak = 148 * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
+    fp32_nominal = 148 * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
+    fp32_peak = fp32_peak_live
     fp32_ach = FLOPS_PER_UPDATE * updates / (launch_ms / 1e3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
@@ -654,14 +708,18 @@ def main():
                      "bytes_per_update": BYTES_PER_UPDATE},
         "fp32_roofline": {"achieved": fp32_ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": fp32_ach / fp32_peak,
                           "flops_per_update": FLOPS_PER_UPDATE,
-                          "peak_source": f"148 SMs x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (nominal, no measured "
-                                         f"FP32 peak on this pool)",
+                          "peak_source": "measured in this run (p2z_measure_peaks): independent FMA chains on "
+                                         "every lane of every SM, the faster of scalar FFMA "
+                                         f"({live_peaks['fp32_ffma_tflops']:.1f}) and paired FFMA2 "
+                                         f"({live_peaks['fp32_ffma2_tflops']:.1f} TFLOP/s)",
+                          "nominal": fp32_nominal,
                           "reference_form": {
                               "flops_per_update": FLOPS_PER_UPDATE_REFERENCE_FORM,
                               "frac": FLOPS_PER_UPDATE_REFERENCE_FORM * updates / (launch_ms / 1e3) / 1e12 / fp32_peak,
                               "note": "the update counted as the reference writes it, products with the "
                                       "Jacobian's known zeros included; this kernel does not execute those"}},
         "clocks": clk,
+        "measured_peaks": live_peaks,
         "autotune": tune_head,
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,

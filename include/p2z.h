@@ -123,6 +123,20 @@ typedef enum p2z_layout {
                                        offset from its anchor; sincosf beyond 0.5 rad) */
 #define P2Z_FLAG_FULL_HITS    0x10u /* p2z_run: copy all 9 hit words per track even for the 2-D
                                        updates (default: only the 6 words they read) */
+#define P2Z_FLAG_PER_EVENT_STREAMS 0x40u /* PER_EVENT: issue the per-event launches round-robin on 10
+                                       streams forked from the run's stream and joined back to it, as
+                                       the reference's GPU build spreads its launches over num_streams
+                                       = 10 (src/propagate-toz-test_CUDA_v4.cu:40-41, :972-986); the
+                                       default issues them in order on the run's stream */
+#define P2Z_FLAG_SORT_WINDOWS 0x80u /* masked runs, FLAT / PERSISTENT: process each window of 256
+                                       consecutive slots in order of the slots' hit counts (a 1-byte
+                                       permutation the run computes on the device), so a warp's 32
+                                       tracks take similar numbers of steps.  Per-track results are
+                                       the same.  Off by default: on the uneven benchmark sample the
+                                       lanes' scattered loads cost more than the 60% -> 92% lane
+                                       utilisation saves (measured slower); packing an event's tracks
+                                       in order of hit count when the arrays are built gains without
+                                       that cost */
 #define P2Z_FLAG_REFERENCE_ROUNDING 0x20u /* P2Z_UPDATE_V2 only: evaluate the reference's own FP32
                                        expressions, type promotions and operation order, every
                                        operation separately rounded, with correctly rounded
@@ -321,6 +335,32 @@ typedef struct p2z_ahit { float pos[3]; float cov[6]; } p2z_ahit;
 p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
                        int64_t ntrks, int nlayer, double smear, double cov_scale, void *trk_out, void *hits_out);
 
+/* The reference's random stream, resumable: the C library's rand() after
+ * srand(seed) (glibc's additive generator, restated) and the reference's
+ * polar-method randn (src/propagate-toz-test_OMP.cpp:127-145), whose second
+ * variate of a pair is kept for the next call.  A plain struct: copy it to
+ * fork the stream.  p2z_prepare is p2z_ref_rng_seed(1), p2z_prepare_tracks,
+ * p2z_prepare_hits on one stream, as the reference's main calls
+ * prepareTracks then prepareHits (:715-720). */
+typedef struct p2z_ref_rng {
+  uint32_t ring[31];     /* the generator's last 31 words */
+  int32_t have_second;   /* randn holds the second variate of a pair */
+  int64_t next;          /* index of the next word */
+  float second;
+  int32_t reserved;
+} p2z_ref_rng;
+void p2z_ref_rng_seed(p2z_ref_rng *g, uint32_t seed);  /* srand(seed) */
+int32_t p2z_ref_rng_rand(p2z_ref_rng *g);               /* rand() */
+float p2z_ref_rng_randn(p2z_ref_rng *g);                /* randn(0, 1) */
+/* prepareTracks (:243-263) on the stream g: nevts*ntrks/bsize MPTRK (host),
+ * every element times (1 + smear*randn), covariance also times cov_scale. */
+p2z_status p2z_prepare_tracks(p2z_ref_rng *g, const p2z_atrk *seed, int bsize, int64_t nevts, int64_t ntrks,
+                              double smear, double cov_scale, void *trk_out);
+/* prepareHits (:265-293) on the stream g: nlayer*nevts*ntrks/bsize MPHIT
+ * (host), layer l from hit seed l; nseeds < nlayer is P2Z_BAD_ARG. */
+p2z_status p2z_prepare_hits(p2z_ref_rng *g, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
+                            int64_t ntrks, int nlayer, double smear, void *hits_out);
+
 /* Physics workload generator (no counterpart in the reference): tracks of
  * charge +-1, pT log-uniform in [pt_min, pt_max] GeV, phi ~ U(-pi, pi),
  * eta ~ U(eta_min, eta_max), vertex z ~ N(0, sigma_vz); covariance
@@ -494,11 +534,40 @@ p2z_status p2z_server_replay(p2z_server *srv, int64_t nreq, const void *const *t
                              const uint32_t *const *hit_mask, const int64_t *ntrks, void *const *trk_out,
                              const double *arrival_s, p2z_request_info *infos);
 
+/* ---- measured roofline denominators (no counterpart in the reference) ------ */
+
+/* Throughputs of the current GPU and its host link, as the benchmark divides by:
+ * FP32 fused multiply-adds (independent chains on every lane of every SM, 64
+ * warps per SM) issued as scalar FFMA and as paired FP32x2 FFMA2, in TFLOP/s
+ * (an FMA is 2 flops); pinned host->device, device->host and both at once
+ * (two streams; the sum of the two directions), in GB/s, for one copy of
+ * copy_bytes (0 -> 1 GiB) each way.  Best of `reps` (0 -> 5) after one
+ * warm-up.  Allocates its own buffers; changes no GPU setting.  device < 0:
+ * the current device.  Synchronous. */
+typedef struct p2z_peaks {
+  double fp32_ffma_tflops;
+  double fp32_ffma2_tflops;
+  double h2d_gbs, d2h_gbs, bidir_gbs;
+  int64_t copy_bytes;
+  int32_t sms;
+} p2z_peaks;
+p2z_status p2z_measure_peaks(int device, size_t copy_bytes, int reps, p2z_peaks *out);
+
 /* ---- host memory helpers ---------------------------------------------------- */
 
 /* Page-locked host allocation (cudaHostAlloc) for fast asynchronous copies. */
 p2z_status p2z_host_alloc(void **ptr, size_t bytes);
 p2z_status p2z_host_free(void *ptr);
+
+/* Device memory on the context's device, for callers without the CUDA
+ * runtime of their own (the typed C++ layer, include/p2z_types.hpp):
+ * cudaMalloc / cudaFree, and a copy in any direction between host and device
+ * pointers (unified addressing) that returns when the copy is complete.  No
+ * counterpart in the reference, whose GPU builds call the CUDA runtime in main
+ * (src/propagate-toz-test_CUDA_v4.cu:921-947). */
+p2z_status p2z_device_alloc(p2z_context *ctx, void **d_ptr, size_t bytes);
+p2z_status p2z_device_free(p2z_context *ctx, void *d_ptr);
+p2z_status p2z_copy(p2z_context *ctx, void *dst, const void *src, size_t bytes);
 
 #ifdef __cplusplus
 }  /* extern "C" */

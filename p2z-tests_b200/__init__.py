@@ -52,6 +52,8 @@ FLAG_NO_GRAPH = 0x4
 FLAG_ACCURATE_TRIG = 0x8
 FLAG_FULL_HITS = 0x10
 FLAG_REFERENCE_ROUNDING = 0x20
+FLAG_PER_EVENT_STREAMS = 0x40
+FLAG_SORT_WINDOWS = 0x80
 
 
 class P2zError(RuntimeError):
@@ -145,6 +147,14 @@ class RequestInfo(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class Peaks(C.Structure):
+    _fields_ = [("fp32_ffma_tflops", C.c_double), ("fp32_ffma2_tflops", C.c_double), ("h2d_gbs", C.c_double),
+                ("d2h_gbs", C.c_double), ("bidir_gbs", C.c_double), ("copy_bytes", C.c_int64), ("sms", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 # Every symbol include/p2z.h declares, with its ctypes signature.
 _VP, _CVP = C.c_void_p, C.c_void_p
 _SIGS = {
@@ -195,7 +205,18 @@ _SIGS = {
                                       _VP]),
     "p2z_autotune": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, C.c_int, C.POINTER(TuneEntry), C.c_int,
                                C.POINTER(C.c_int), C.POINTER(TuneEntry)]),
+    "p2z_measure_peaks": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(Peaks)]),
     "p2z_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
+    "p2z_device_alloc": (C.c_int, [_VP, C.POINTER(C.c_void_p), C.c_size_t]),
+    "p2z_device_free": (C.c_int, [_VP, _VP]),
+    "p2z_copy": (C.c_int, [_VP, _VP, _CVP, C.c_size_t]),
+    "p2z_ref_rng_seed": (None, [_VP, C.c_uint32]),
+    "p2z_ref_rng_rand": (C.c_int32, [_VP]),
+    "p2z_ref_rng_randn": (C.c_float, [_VP]),
+    "p2z_prepare_tracks": (C.c_int, [_VP, C.POINTER(Atrk), C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                     _VP]),
+    "p2z_prepare_hits": (C.c_int, [_VP, C.POINTER(Ahit), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int,
+                                   C.c_double, _VP]),
     "p2z_host_free": (C.c_int, [_VP]),
 }
 
@@ -227,6 +248,14 @@ def _check(status: int, ctx=None):
     if status != OK:
         msg = lib.p2z_last_error(ctx)
         raise P2zError(status, (msg or b"").decode())
+
+
+def measure_peaks(device=-1, copy_bytes=0, reps=0) -> dict:
+    """FP32 FMA throughput (TFLOP/s) and pinned copy rates (GB/s) of the GPU
+    (p2z_measure_peaks)."""
+    pk = Peaks()
+    _check(lib.p2z_measure_peaks(device, copy_bytes, reps, C.byref(pk)))
+    return pk.as_dict()
 
 
 def version() -> str:

@@ -19,6 +19,17 @@
 #ifndef P2Z_RUN_MAX_CHUNKS
 #define P2Z_RUN_MAX_CHUNKS 8
 #endif
+// P2Z_FLAG_PER_EVENT_STREAMS: streams the per-event launches are spread over.
+constexpr int kEventStreams = 10;
+// Masked runs with P2Z_FLAG_SORT_WINDOWS: slots per sorted window.
+// A warp's 32 tracks take as many steps as the longest of them; with hit
+// counts of 5-20 per track, 32 slots taken in stored order keep 60% of the
+// lane-steps busy, 256 slots sorted by hit count 92% (32 sorted slots, i.e.
+// no sort, 60%; 64: 74%; 128: 85%).  The window stays within 8 batches of 32,
+// so a warp's loads stay within that many neighbouring batches.
+#ifndef P2Z_SORT_WINDOW
+#define P2Z_SORT_WINDOW 256
+#endif
 
 namespace p2z {
 cudaError_t launch_step(int bsize, float *trk, const float *hits, int64_t nslots, int nlayer, int layer, int what,
@@ -64,10 +75,13 @@ struct p2z_context {
   unsigned long long *d_queue = nullptr;    // 2 persistent work counters (one per copy stream)
   DevBuf trk, hits, out, mask, valid;       // p2z_run buffers / internal masks
   DevBuf aux;                               // scratch of the validation reduction
+  DevBuf perm;                              // sorted-window permutation (masked runs)
   bool has_graph = false;
   GraphKey gkey;
   cudaGraphExec_t gexec = nullptr;
   std::vector<Tuned> tuned;                 // p2z_autotune results
+  cudaStream_t ev_streams[kEventStreams] = {};  // P2Z_FLAG_PER_EVENT_STREAMS (created on first use)
+  cudaEvent_t ev_fork = nullptr, ev_join[kEventStreams] = {};
   std::string last_error;
 };
 
@@ -232,6 +246,38 @@ __global__ void k_count_updates(const uint32_t *mask, int64_t nslots, uint32_t a
 
 uint32_t all_layers(int nlayer) { return nlayer >= 32 ? 0xffffffffu : ((1u << nlayer) - 1u); }
 
+// One CTA per window of `win` slots of [s0, s1): a counting sort of the
+// window's slots by hit count, most hits first, written as the within-window
+// offset of the slot each rank processes (perm[window base + rank]).  Ranks
+// of equal hit count are assigned by shared-memory atomics, so which thread
+// processes which of them varies from run to run; every track's arithmetic
+// is independent of its thread, so the results do not.
+__global__ void __launch_bounds__(P2Z_SORT_WINDOW) k_sort_windows(const uint32_t *__restrict__ mask, uint8_t *perm,
+                                                                  int64_t s0, int64_t s1, int win, uint32_t all) {
+  __shared__ int hist[33];
+  __shared__ int start[33];
+  const int i = threadIdx.x;
+  const int64_t base = s0 + (int64_t)blockIdx.x * win;
+  const int n = (int)min((int64_t)win, s1 - base);
+  if (i < 33) hist[i] = 0;
+  __syncthreads();
+  int key = 0, pos = 0;
+  if (i < n) {
+    key = 32 - __popc(__ldg(mask + base + i) & all);  // 0 = all 32 layers present
+    pos = atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  if (i == 0) {
+    int acc = 0;
+    for (int k = 0; k < 33; ++k) {
+      start[k] = acc;
+      acc += hist[k];
+    }
+  }
+  __syncthreads();
+  if (i < n) perm[base + start[key] + pos] = (uint8_t)i;
+}
+
 // Enqueue the hot-path launches of one pass over slots [s0, s1) on st.
 // queue: the persistent work counter to use.
 p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, int64_t s0, int64_t s1,
@@ -249,21 +295,56 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   spec.grid = 0;
   if (schedule == P2Z_SCHED_PER_EVENT) {
     spec.kind = KIND_FLAT;
+    const bool spread = (pl.flags & P2Z_FLAG_PER_EVENT_STREAMS) != 0;
+    if (spread) {
+      if (!ctx->ev_fork) {
+        P2Z_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+        for (int i = 0; i < kEventStreams; ++i) {
+          P2Z_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->ev_streams[i], cudaStreamNonBlocking));
+          P2Z_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming));
+        }
+      }
+      P2Z_CUDA(ctx, cudaEventRecord(ctx->ev_fork, st));
+      for (int i = 0; i < kEventStreams; ++i) P2Z_CUDA(ctx, cudaStreamWaitEvent(ctx->ev_streams[i], ctx->ev_fork, 0));
+    }
     const int64_t nev = (int64_t)pl.ev_slot_begin.size() - 1;
+    int k = 0;
     for (int64_t e = 0; e < nev; ++e) {
       const int64_t a = std::max(s0, pl.ev_slot_begin[e]), b = std::min(s1, pl.ev_slot_begin[e + 1]);
       if (b <= a) continue;
       spec.args.slot_begin = a;
       spec.args.slot_end = b;
-      P2Z_CUDA(ctx, dispatch(spec, st));
+      P2Z_CUDA(ctx, dispatch(spec, spread ? ctx->ev_streams[k++ % kEventStreams] : st));
       ++*launches;
+    }
+    if (spread) {
+      for (int i = 0; i < kEventStreams; ++i) {
+        P2Z_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->ev_streams[i]));
+        P2Z_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_join[i], 0));
+      }
     }
     return P2Z_OK;
   }
   spec.args.slot_begin = s0;
   spec.args.slot_end = s1;
   if (s1 <= s0) return P2Z_OK;
+  // masked flat and persistent runs: process each window's slots in order of hit count
+  const bool sort = spec.masked && (pl.flags & P2Z_FLAG_SORT_WINDOWS) &&
+                    (schedule == P2Z_SCHED_FLAT || schedule == P2Z_SCHED_PERSISTENT);
+  if (sort) {
+    p2z_status r = ensure(ctx, ctx->perm, (size_t)pl.nslots);
+    if (r != P2Z_OK) return r;
+    spec.args.perm = (const uint8_t *)ctx->perm.p;
+    spec.args.win = P2Z_SORT_WINDOW;
+  }
+  auto launch_sort = [&](cudaStream_t s) {
+    const int64_t nwin = (s1 - s0 + P2Z_SORT_WINDOW - 1) / P2Z_SORT_WINDOW;
+    k_sort_windows<<<(unsigned)nwin, P2Z_SORT_WINDOW, 0, s>>>(base.mask, (uint8_t *)ctx->perm.p, s0, s1,
+                                                               P2Z_SORT_WINDOW, all_layers(pl.nlayer));
+    return cudaGetLastError();
+  };
   if (schedule == P2Z_SCHED_FLAT) {
+    if (sort) P2Z_CUDA(ctx, launch_sort(st));
     spec.kind = KIND_FLAT;
     P2Z_CUDA(ctx, dispatch(spec, st));
     ++*launches;
@@ -284,6 +365,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   P2Z_CUDA(ctx, cudaStreamIsCapturing(st, &cap));
   const bool use_graph = !(pl.flags & P2Z_FLAG_NO_GRAPH) && cap == cudaStreamCaptureStatusNone;
   if (!use_graph) {
+    if (sort) P2Z_CUDA(ctx, launch_sort(st));
     P2Z_CUDA(ctx, cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
     P2Z_CUDA(ctx, dispatch(spec, st));
     ++*launches;
@@ -312,7 +394,9 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
     cudaGraph_t g = nullptr;
     cudaStream_t cs = ctx->stream;
     P2Z_CUDA(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e0 = sort ? launch_sort(cs) : cudaSuccess;
     cudaError_t e1 = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), cs);
+    if (e1 == cudaSuccess) e1 = e0;
     cudaError_t e2 = dispatch(spec, cs);
     cudaError_t e3 = cudaStreamEndCapture(cs, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
@@ -534,12 +618,19 @@ p2z_status p2z_destroy(p2z_context *c) {
   for (int i = 0; i < 2; ++i)
     if (c->copy[i]) cudaStreamSynchronize(c->copy[i]);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
-  for (DevBuf *b : {&c->trk, &c->hits, &c->out, &c->mask, &c->valid, &c->aux})
+  for (DevBuf *b : {&c->trk, &c->hits, &c->out, &c->mask, &c->valid, &c->aux, &c->perm})
     if (b->p) cudaFree(b->p);
   if (c->d_status) cudaFree(c->d_status);
   if (c->d_queue) cudaFree(c->d_queue);
-  for (cudaEvent_t ev : {c->ev0, c->ev1, c->ev2, c->ev3, c->join[0], c->join[1]})
+  for (cudaEvent_t ev : {c->ev0, c->ev1, c->ev2, c->ev3, c->join[0], c->join[1], c->ev_fork})
     if (ev) cudaEventDestroy(ev);
+  for (int i = 0; i < kEventStreams; ++i) {
+    if (c->ev_streams[i]) {
+      cudaStreamSynchronize(c->ev_streams[i]);
+      cudaStreamDestroy(c->ev_streams[i]);
+    }
+    if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
+  }
   for (int i = 0; i < 2; ++i)
     if (c->copy[i]) cudaStreamDestroy(c->copy[i]);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -759,6 +850,33 @@ p2z_status p2z_host_alloc(void **ptr, size_t bytes) {
     return fail(nullptr, e == cudaErrorMemoryAllocation ? P2Z_OOM : P2Z_CUDA_ERROR, "cudaHostAlloc(%zu): %s", bytes,
                 cudaGetErrorString(e));
   }
+  return P2Z_OK;
+}
+
+p2z_status p2z_device_alloc(p2z_context *ctx, void **d_ptr, size_t bytes) {
+  if (!ctx || !d_ptr) return fail(ctx, P2Z_BAD_ARG, "context or pointer is NULL");
+  *d_ptr = nullptr;
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  P2Z_CUDA(ctx, cudaMalloc(d_ptr, bytes ? bytes : 1));
+  return P2Z_OK;
+}
+
+p2z_status p2z_device_free(p2z_context *ctx, void *d_ptr) {
+  if (!ctx) return fail(nullptr, P2Z_BAD_ARG, "context is NULL");
+  if (!d_ptr) return P2Z_OK;
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  P2Z_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  P2Z_CUDA(ctx, cudaFree(d_ptr));
+  return P2Z_OK;
+}
+
+p2z_status p2z_copy(p2z_context *ctx, void *dst, const void *src, size_t bytes) {
+  if (!ctx) return fail(nullptr, P2Z_BAD_ARG, "context is NULL");
+  if (bytes == 0) return P2Z_OK;
+  if (!dst || !src) return fail(ctx, P2Z_BAD_ARG, "NULL copy pointer");
+  P2Z_CUDA(ctx, cudaSetDevice(ctx->device));
+  P2Z_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+  P2Z_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return P2Z_OK;
 }
 

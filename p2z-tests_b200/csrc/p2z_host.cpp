@@ -15,6 +15,7 @@
 
 #include "p2z.h"
 #include "p2z_gen.h"
+#include "p2z_refrng.h"
 
 namespace {
 
@@ -22,55 +23,6 @@ constexpr int TRK_WORDS = 28;
 constexpr int HIT_WORDS = 9;
 
 bool valid_bsize(int b) { return b == 8 || b == 16 || b == 32 || b == 64; }
-
-// ---------------------------------------------------------------------------
-// Reference-compatible Gaussian stream
-// ---------------------------------------------------------------------------
-// The reference draws every smearing factor from randn (src/propagate-toz-
-// test_OMP.cpp:127-145): Marsaglia's polar method on the C library's rand(),
-// returning the two variates of an accepted pair on consecutive calls.  Types
-// follow the reference exactly: U = -1 + (float)rand()/RAND_MAX*2 in float,
-// W = pow(U1,2) + pow(U2,2) in double stored to float, mult = sqrtf(-2*logf(W)/W).
-// rand() after srand(1) is glibc's additive-feedback random(); random_r on a
-// private TYPE_3 state seeded with 1 yields the same sequence without touching
-// the process-wide generator.
-class RefGauss {
- public:
-  RefGauss() {
-    std::memset(&rd_, 0, sizeof rd_);
-    std::memset(state_, 0, sizeof state_);
-    initstate_r(1u, state_, sizeof state_, &rd_);
-    srandom_r(1u, &rd_);
-  }
-  float next() {
-    if (have_second_) {
-      have_second_ = false;
-      return 0.f + 1.f * x2_;
-    }
-    float u1, u2, w;
-    do {
-      u1 = -1 + ((float)draw() / RAND_MAX) * 2;
-      u2 = -1 + ((float)draw() / RAND_MAX) * 2;
-      w = (float)((double)u1 * (double)u1 + (double)u2 * (double)u2);
-    } while (w >= 1 || w == 0);
-    const float mult = sqrtf((-2 * logf(w)) / w);
-    x1_ = u1 * mult;
-    x2_ = u2 * mult;
-    have_second_ = true;
-    return 0.f + 1.f * x1_;
-  }
-
- private:
-  int32_t draw() {
-    int32_t r = 0;
-    random_r(&rd_, &r);
-    return r;
-  }
-  struct random_data rd_;
-  char state_[128];
-  float x1_ = 0.f, x2_ = 0.f;
-  bool have_second_ = false;
-};
 
 // The reference's smearing factor (1 + smear*randn), formed in double.  Its
 // builds compile with FMA contraction on (gcc -O3 -march=native), which turns
@@ -104,28 +56,46 @@ void parallel_for(int64_t n, int nthr, F f) {
 
 extern "C" {
 
-p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
-                       int64_t ntrks, int nlayer, double smear, double cov_scale, void *trk_out, void *hits_out) {
-  if (!seed || !hit_seeds || !trk_out || !hits_out) return P2Z_BAD_ARG;
+void p2z_ref_rng_seed(p2z_ref_rng *g, uint32_t seed) {
+  if (g) p2z_refrng::seed(g, seed);
+}
+
+int32_t p2z_ref_rng_rand(p2z_ref_rng *g) { return g ? p2z_refrng::draw(g) : -1; }
+
+float p2z_ref_rng_randn(p2z_ref_rng *g) { return g ? p2z_refrng::randn(g) : NAN; }
+
+p2z_status p2z_prepare_tracks(p2z_ref_rng *g, const p2z_atrk *seed, int bsize, int64_t nevts, int64_t ntrks,
+                              double smear, double cov_scale, void *trk_out) {
+  if (!g || !seed || (!trk_out && nevts * ntrks > 0)) return P2Z_BAD_ARG;
   if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
-  if (nevts < 0 || ntrks < 0 || ntrks % bsize || nlayer < 1 || nlayer > 32) return P2Z_BAD_ARG;
-  if (nseeds < nlayer) return P2Z_BAD_ARG;  // the reference exits here (:271-274)
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize) return P2Z_BAD_ARG;
   const int64_t nb = ntrks / bsize;
   float *T = (float *)trk_out;
-  float *H = (float *)hits_out;
-  RefGauss g;
-  // prepareTracks (:243-263): event, batch, lane; 6 parameters then 21
-  // covariance elements, each scaled by (1 + smear*randn); cov also * cov_scale.
+  // prepareTracks (src/propagate-toz-test_OMP.cpp:243-263): event, batch,
+  // lane; 6 parameters then 21 covariance elements, each scaled by
+  // (1 + smear*randn); covariance also by cov_scale (100 in the reference);
+  // the charge copied.
   for (int64_t ie = 0; ie < nevts; ++ie)
     for (int64_t ib = 0; ib < nb; ++ib) {
       float *b = T + (ib + nb * ie) * (int64_t)TRK_WORDS * bsize;
       for (int it = 0; it < bsize; ++it) {
-        for (int ip = 0; ip < 6; ++ip) b[it + ip * bsize] = smear_factor(smear, g.next()) * seed->par[ip];
+        for (int ip = 0; ip < 6; ++ip) b[it + ip * bsize] = smear_factor(smear, p2z_refrng::randn(g)) * seed->par[ip];
         for (int ip = 0; ip < 21; ++ip)
-          b[6 * bsize + it + ip * bsize] = smear_factor(smear, g.next()) * seed->cov[ip] * cov_scale;
+          b[6 * bsize + it + ip * bsize] = smear_factor(smear, p2z_refrng::randn(g)) * seed->cov[ip] * cov_scale;
         std::memcpy(&b[27 * bsize + it], &seed->q, sizeof(int32_t));
       }
     }
+  return P2Z_OK;
+}
+
+p2z_status p2z_prepare_hits(p2z_ref_rng *g, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
+                            int64_t ntrks, int nlayer, double smear, void *hits_out) {
+  if (!g || !hit_seeds || (!hits_out && nevts * ntrks > 0)) return P2Z_BAD_ARG;
+  if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize || nlayer < 1 || nlayer > 32) return P2Z_BAD_ARG;
+  if (nseeds < nlayer) return P2Z_BAD_ARG;  // the reference exits here (:271-274)
+  const int64_t nb = ntrks / bsize;
+  float *H = (float *)hits_out;
   // prepareHits (:265-293): layer outermost; layer l of batch ib of event ie
   // at hit batch l + nlayer*(ib + nb*ie).
   for (int lay = 0; lay < nlayer; ++lay) {
@@ -134,12 +104,28 @@ p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nsee
       for (int64_t ib = 0; ib < nb; ++ib) {
         float *h = H + (lay + nlayer * (ib + nb * ie)) * (int64_t)HIT_WORDS * bsize;
         for (int it = 0; it < bsize; ++it) {
-          for (int ip = 0; ip < 3; ++ip) h[it + ip * bsize] = smear_factor(smear, g.next()) * s.pos[ip];
-          for (int ip = 0; ip < 6; ++ip) h[3 * bsize + it + ip * bsize] = smear_factor(smear, g.next()) * s.cov[ip];
+          for (int ip = 0; ip < 3; ++ip) h[it + ip * bsize] = smear_factor(smear, p2z_refrng::randn(g)) * s.pos[ip];
+          for (int ip = 0; ip < 6; ++ip)
+            h[3 * bsize + it + ip * bsize] = smear_factor(smear, p2z_refrng::randn(g)) * s.cov[ip];
         }
       }
   }
   return P2Z_OK;
+}
+
+p2z_status p2z_prepare(const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
+                       int64_t ntrks, int nlayer, double smear, double cov_scale, void *trk_out, void *hits_out) {
+  if (!seed || !hit_seeds || !trk_out || !hits_out) return P2Z_BAD_ARG;
+  if (!valid_bsize(bsize)) return P2Z_UNSUPPORTED;
+  if (nevts < 0 || ntrks < 0 || ntrks % bsize || nlayer < 1 || nlayer > 32) return P2Z_BAD_ARG;
+  if (nseeds < nlayer) return P2Z_BAD_ARG;
+  // the reference's main: rand() in its initial state (srand(1)), then
+  // prepareTracks, then prepareHits on the same stream (:715-720)
+  p2z_ref_rng g;
+  p2z_refrng::seed(&g, 1u);
+  p2z_status r = p2z_prepare_tracks(&g, seed, bsize, nevts, ntrks, smear, cov_scale, trk_out);
+  if (r != P2Z_OK) return r;
+  return p2z_prepare_hits(&g, hit_seeds, nseeds, bsize, nevts, ntrks, nlayer, smear, hits_out);
 }
 
 void p2z_physics_defaults(p2z_physics_params *p) {

@@ -75,7 +75,19 @@ struct RunArgs {
   unsigned int *status;            // bit 0: a det <= 0 was met; bit 1: a staging wait timed out
   unsigned long long *queue;       // persistent kernels: next work item
   int64_t ws;                      // SoA layout (B == 0): slots in the arrays = word stride
+  // Sorted windows (masked runs): the launch's slots are split into windows
+  // of `win` slots from slot_begin; the thread at linear slot s processes
+  // slot window_base(s) + perm[s].  perm == nullptr: s itself.
+  const uint8_t *__restrict__ perm;
+  int win;                         // slots per window, a power of two <= 256
 };
+
+// The slot a thread processes (see RunArgs::perm).
+__device__ __forceinline__ int64_t map_slot(const RunArgs &a, int64_t s) {
+  if (a.perm == nullptr) return s;
+  const int64_t base = a.slot_begin + ((s - a.slot_begin) & ~(int64_t)(a.win - 1));
+  return base + __ldg(a.perm + s);
+}
 
 // Layouts.  B > 0: the reference's AOSOA batches of width B (element e of a
 // lane at e*B from the lane's first word).  B == 0: SoA -- one batch as wide as
@@ -149,10 +161,10 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
     const float hp[3] = {h.w[0], h.w[1], h.w[2]};
     if constexpr (UPD == UPDK_V2 || UPD == UPDK_V2_REF) {
       const float hc[3] = {h.w[3], h.w[4], h.w[5]};
-      return update_v2<typename Types<UPD>::A, (UPD == UPDK_V2_REF) ? FORM_REFERENCE : FORM_PRECISE>(s, hp, hc);
+      return update_v2<typename Types<UPD>::A, (UPD == UPDK_V2_REF) ? FORM_REFERENCE : FORM_PRECISE, GENERAL>(s, hp, hc);
     } else if constexpr (UPD == UPDK_V2_COMP) {
       const float hc[3] = {h.w[3], h.w[4], h.w[5]};
-      return update_v2<DF, FORM_PRECISE>(s, hp, hc);
+      return update_v2<DF, FORM_PRECISE, GENERAL>(s, hp, hc);
     } else {
       const float hv[6] = {h.w[3], h.w[4], h.w[5], h.w[6], h.w[7], h.w[8]};
       if constexpr (UPD == UPDK_3X3_F64) return update_3x3_joseph<double>(s, hp, hv);
@@ -292,7 +304,7 @@ template <int B, int UPD, int SC, bool MASKED>
 __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_flat(RunArgs a) {
   const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= a.slot_end) return;
-  process_slot<B, UPD, SC, MASKED>(a, slot);
+  process_slot<B, UPD, SC, MASKED>(a, map_slot(a, slot));
 }
 
 // Persistent launch: grid = resident CTAs; each warp repeatedly takes the next
@@ -310,7 +322,7 @@ __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArg
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nitems) break;
     const int64_t slot = a.slot_begin + (int64_t)item * 32 + lane;
-    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, slot);
+    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, map_slot(a, slot));
   }
 }
 

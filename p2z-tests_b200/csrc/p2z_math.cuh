@@ -211,6 +211,15 @@ __device__ __forceinline__ void rotated(float c, float s, float w, float v, floa
 // tan_offset.
 constexpr float kAnchorPhi = 0.4f;
 constexpr float kAnchorTheta = 0.02f;
+// Ranges of the offset evaluations (sv_series: |dP| <= 0.5; tan_offset:
+// |dT| <= 0.2).  An offset beyond them -- after a Kalman correction of more
+// than ~0.1 rad, which only a track whose covariance no longer describes it
+// receives -- or a non-finite one re-anchors the direction at the track's own
+// angles (sincosf, as the first layer does) before the step, so the
+// polynomials are never evaluated outside their range: such a track stays
+// finite wherever the angles themselves are.
+constexpr float kRangePhi = 0.5f;
+constexpr float kRangeTheta = 0.2f;
 
 // ---------------------------------------------------------------------------
 // Track state in registers
@@ -275,6 +284,18 @@ struct Jac {
 
 // ---- FORM_PRECISE -----------------------------------------------------------
 
+// First evaluation of the carried direction of a track: the anchors at the
+// input angles, zero offsets.
+template <typename A>
+__device__ __forceinline__ void init_direction(Trk<float, A> &s) {
+  sincosf(tof(s.phi), &s.sP, &s.cP);
+  float sT, cT;
+  sincosf(s.theta, &sT, &cT);
+  s.tT = __fdiv_rn(sT, cT);
+  s.dP = 0.f;
+  s.dT = 0.f;
+}
+
 // Parameter propagation (reference :627-647), with the reference's products
 // regrouped around shared factors (exact in real arithmetic):
 //   alpha = deltaZ*sinT*ipt*icosT/k = (deltaZ/k)*tanT*ipt,
@@ -296,6 +317,7 @@ struct Jac {
 template <int SC, typename A>
 __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &s, float zout, float k, float ik) {
   Helix<float> h;
+  if (__builtin_expect(!(fabsf(s.dP) <= kRangePhi && fabsf(s.dT) <= kRangeTheta), 0)) init_direction(s);
   h.deltaZ = zout - s.z;
   h.pt = rcp_nr(s.ipt);
   {
@@ -334,18 +356,6 @@ __device__ __forceinline__ Helix<float> propagate_params_precise(Trk<float, A> &
   s.sP = moveP ? sPn : s.sP;
   s.dP = moveP ? 0.f : dP;
   return h;
-}
-
-// First evaluation of the carried direction of a track: the anchors at the
-// input angles, zero offsets.
-template <typename A>
-__device__ __forceinline__ void init_direction(Trk<float, A> &s) {
-  sincosf(tof(s.phi), &s.sP, &s.cP);
-  float sT, cT;
-  sincosf(s.theta, &sT, &cT);
-  s.tT = __fdiv_rn(sT, cT);
-  s.dP = 0.f;
-  s.dT = 0.f;
 }
 
 // A Kalman correction of phi and theta, added to the offsets from the
@@ -618,20 +628,43 @@ __device__ __forceinline__ float det2_comp(float a, float b, float c, float d) {
 
 // Apply the 2-D (x,y) gain: K(i,:) = (C(i,0), C(i,1)) * Rinv for the live rows
 // (the z row is zero), the parameter update with the residual (hx - x,
-// hy - y), and C - K (H C) (reference :534-617).
+// hy - y), and the covariance update, C - K H C (reference :534-617).
 // FORM_PRECISE, FP32 with packed pairs: the gain rows (K_i0, K_i1) as
-// c_i0 (r00, r01) + c_i1 (r01, r11), and C - K (H C) with the column-0/1 pairs
-// of rows y, ipt, phi, theta updated together:
-//   (c_i0, c_i1)' = (c_i0, c_i1) - K_i0 (c00, c10) - K_i1 (c10, c11).
-template <typename A>
-__device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r00, float r01, float r11, float hx,
-                                                       float hy) {
-  const float2 R0 = make_float2(r00, r01), R1 = make_float2(r01, r11);
-  const float2 Kx = fma2(bc2(s.c10), R1, mul2(bc2(s.c00), R0));  // (K0, K1)
-  const float2 Ky = fma2(bc2(s.c11), R1, mul2(bc2(s.c10), R0));  // (K2, K3)
-  const float2 Ki = fma2(bc2(s.c31), R1, mul2(bc2(s.c30), R0));  // (K6, K7)
-  const float2 Kp = fma2(bc2(s.c41), R1, mul2(bc2(s.c40), R0));  // (K8, K9)
-  const float2 Kt = fma2(bc2(s.c51), R1, mul2(bc2(s.c50), R0));  // (K10, K11)
+// c_i0 (i00, i01) + c_i1 (i01, i11); rows x, y, ipt, phi, theta of C's
+// measured columns as pairs B_i = (c_i0, c_i1); A = the measured 2x2 block.
+//
+// C - K H C subtracts nearly equal numbers where the update shrinks C by a
+// large factor in some direction, and there a gain rounded by a few ulp (its
+// relative error grows with R's condition number) costs many digits: on a
+// track whose first hit is 200x more precise than the track in one
+// direction, C then stops describing the track, and the gains of later
+// layers with it.  That is the first update of a track, where its prior
+// covariance meets a measurement, so a track's first update (FIRST) takes the
+// Joseph form (I-KH) C (I-KH)^T + K V K^T instead, evaluated as
+// C'' = P - E K^T with P = C - K H C and E = P H^T - K V, the residual of the
+// gain equation, which cancels K's rounding errors to first order.  K V is
+// formed from error-free products (p = K0*v, e = fma(K0, v, -p)): with an
+// elongated V (eigenvalues 1e6 apart on the reference's known-answer hits)
+// the two products cancel, and a rounded first product would leave an error
+// of eps*|K||V| in E.  Later updates keep C - K H C: after the first update C
+// is already a fit of the track and an update shrinks it by small factors,
+// where C - K H C is accurate, at 22 instructions against the Joseph form's
+// 69.  Measured on one B200: Joseph on every layer costs 10.8% of the pass,
+// with the same results on every sample tried (single-seed, known-answer,
+// physics and the conditioning sweep); choosing per track by the shrink
+// det(I - K H) costs more than Joseph on every first layer, because physics
+// tracks straddle any threshold and a warp then runs both forms.
+template <bool FIRST, typename A>
+__device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float i00, float i01, float i11, float hx,
+                                                       float hy, float v00, float v01, float v11) {
+  const float2 I0 = make_float2(i00, i01), I1 = make_float2(i01, i11);
+  const float2 A0 = make_float2(s.c00, s.c10), A1 = make_float2(s.c10, s.c11);
+  const float2 B3 = make_float2(s.c30, s.c31), B4 = make_float2(s.c40, s.c41), B5 = make_float2(s.c50, s.c51);
+  const float2 Kx = fma2(bc2(s.c10), I1, mul2(bc2(s.c00), I0));  // (K0, K1)
+  const float2 Ky = fma2(bc2(s.c11), I1, mul2(bc2(s.c10), I0));  // (K2, K3)
+  const float2 Ki = fma2(bc2(B3.y), I1, mul2(bc2(B3.x), I0));  // (K6, K7)
+  const float2 Kp = fma2(bc2(B4.y), I1, mul2(bc2(B4.x), I0));  // (K8, K9)
+  const float2 Kt = fma2(bc2(B5.y), I1, mul2(bc2(B5.x), I0));  // (K10, K11)
   const float res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
   acc_update(s.x, hx, res0, Kx.x * res0 + Kx.y * res1);
   acc_update(s.y, hy, res1, Ky.x * res0 + Ky.y * res1);
@@ -641,31 +674,65 @@ __device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r
   s.theta = __fadd_rn(s.theta, dth);
   turn_direction(s, dphi, dth);
   s.ipt = s.ipt + Ki.x * res0 + Ki.y * res1;
-  const float2 P0 = make_float2(s.c00, s.c10), Q = make_float2(s.c10, s.c11);
-  const float c30 = s.c30, c31 = s.c31, c40 = s.c40, c41 = s.c41, c50 = s.c50, c51 = s.c51;
-  s.c00 = fmaf(-Kx.y, s.c10, fmaf(-Kx.x, s.c00, s.c00));
-  const float2 Ny = fma2(bc2(-Ky.y), Q, fma2(bc2(-Ky.x), P0, Q));
-  const float2 Ni = fma2(bc2(-Ki.y), Q, fma2(bc2(-Ki.x), P0, make_float2(c30, c31)));
-  const float2 Np = fma2(bc2(-Kp.y), Q, fma2(bc2(-Kp.x), P0, make_float2(c40, c41)));
-  const float2 Nt = fma2(bc2(-Kt.y), Q, fma2(bc2(-Kt.x), P0, make_float2(c50, c51)));
+  // P = C - K H C on the measured columns of every live row
+  const float2 Px = fma2(bc2(-Kx.y), A1, fma2(bc2(-Kx.x), A0, A0));
+  const float2 Py = fma2(bc2(-Ky.y), A1, fma2(bc2(-Ky.x), A0, A1));
+  const float2 Pi = fma2(bc2(-Ki.y), A1, fma2(bc2(-Ki.x), A0, B3));
+  const float2 Pp = fma2(bc2(-Kp.y), A1, fma2(bc2(-Kp.x), A0, B4));
+  const float2 Pt = fma2(bc2(-Kt.y), A1, fma2(bc2(-Kt.x), A0, B5));
+  if constexpr (!FIRST) {
+    s.c00 = Px.x;
+    s.c10 = Py.x; s.c11 = Py.y;
+    s.c30 = Pi.x; s.c31 = Pi.y;
+    s.c40 = Pp.x; s.c41 = Pp.y;
+    s.c50 = Pt.x; s.c51 = Pt.y;
+    s.c33 = fmaf(-Ki.y, B3.y, fmaf(-Ki.x, B3.x, s.c33));
+    s.c43 = fmaf(-Kp.y, B3.y, fmaf(-Kp.x, B3.x, s.c43));
+    s.c44 = fmaf(-Kp.y, B4.y, fmaf(-Kp.x, B4.x, s.c44));
+    s.c53 = fmaf(-Kt.y, B3.y, fmaf(-Kt.x, B3.x, s.c53));
+    s.c54 = fmaf(-Kt.y, B4.y, fmaf(-Kt.x, B4.x, s.c54));
+    s.c55 = fmaf(-Kt.y, B5.y, fmaf(-Kt.x, B5.x, s.c55));
+    return;
+  }
+  // Joseph form: E_i = P_i - K_i V (K V from error-free products), then
+  // C''(i, m) = P(i, m) - E_i . K_m for the measured columns and
+  // C''(a, b) = C(a, b) - K_a . B_b - E_a . K_b on the unmeasured block.
+  const float2 V0 = make_float2(v00, v01), V1 = make_float2(v01, v11);
+  const float2 Kc0 = make_float2(Kx.x, Ky.x), Kc1 = make_float2(Kx.y, Ky.y);
+  auto resid = [&](const float2 P, const float2 K) {
+    const float2 p = mul2(bc2(-K.x), V0);
+    const float2 e = fma2(bc2(-K.x), V0, make_float2(-p.x, -p.y));  // exact: -K0 V0 - p
+    return __fadd2_rn(__fadd2_rn(fma2(bc2(-K.y), V1, p), e), P);
+  };
+  const float2 Ex = resid(Px, Kx), Ey = resid(Py, Ky), Ei = resid(Pi, Ki), Ep = resid(Pp, Kp), Et = resid(Pt, Kt);
+  const float2 Nx = fma2(bc2(-Ex.y), Kc1, fma2(bc2(-Ex.x), Kc0, Px));
+  const float2 Ny = fma2(bc2(-Ey.y), Kc1, fma2(bc2(-Ey.x), Kc0, Py));
+  const float2 Ni = fma2(bc2(-Ei.y), Kc1, fma2(bc2(-Ei.x), Kc0, Pi));
+  const float2 Np = fma2(bc2(-Ep.y), Kc1, fma2(bc2(-Ep.x), Kc0, Pp));
+  const float2 Nt = fma2(bc2(-Et.y), Kc1, fma2(bc2(-Et.x), Kc0, Pt));
+  s.c33 = fmaf(-Ei.y, Ki.y, fmaf(-Ei.x, Ki.x, fmaf(-Ki.y, B3.y, fmaf(-Ki.x, B3.x, s.c33))));
+  s.c43 = fmaf(-Ep.y, Ki.y, fmaf(-Ep.x, Ki.x, fmaf(-Kp.y, B3.y, fmaf(-Kp.x, B3.x, s.c43))));
+  s.c44 = fmaf(-Ep.y, Kp.y, fmaf(-Ep.x, Kp.x, fmaf(-Kp.y, B4.y, fmaf(-Kp.x, B4.x, s.c44))));
+  s.c53 = fmaf(-Et.y, Ki.y, fmaf(-Et.x, Ki.x, fmaf(-Kt.y, B3.y, fmaf(-Kt.x, B3.x, s.c53))));
+  s.c54 = fmaf(-Et.y, Kp.y, fmaf(-Et.x, Kp.x, fmaf(-Kt.y, B4.y, fmaf(-Kt.x, B4.x, s.c54))));
+  s.c55 = fmaf(-Et.y, Kt.y, fmaf(-Et.x, Kt.x, fmaf(-Kt.y, B5.y, fmaf(-Kt.x, B5.x, s.c55))));
+  s.c00 = Nx.x;
   s.c10 = Ny.x; s.c11 = Ny.y;
   s.c30 = Ni.x; s.c31 = Ni.y;
   s.c40 = Np.x; s.c41 = Np.y;
   s.c50 = Nt.x; s.c51 = Nt.y;
-  s.c33 = fmaf(-Ki.y, c31, fmaf(-Ki.x, c30, s.c33));
-  s.c43 = fmaf(-Kp.y, c31, fmaf(-Kp.x, c30, s.c43));
-  s.c44 = fmaf(-Kp.y, c41, fmaf(-Kp.x, c40, s.c44));
-  s.c53 = fmaf(-Kt.y, c31, fmaf(-Kt.x, c30, s.c53));
-  s.c54 = fmaf(-Kt.y, c41, fmaf(-Kt.x, c40, s.c54));
-  s.c55 = fmaf(-Kt.y, c51, fmaf(-Kt.x, c50, s.c55));
 }
 
-template <typename T, typename A, int FORM>
-__device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r11, T hx, T hy) {
+// The generic form (FP64 kernel, reference rounding, unpacked FP32): the
+// reference's C - K (H C).  v (the hit covariance) is used by the packed FP32
+// form only.
+template <typename T, typename A, int FORM, bool FIRST = false>
+__device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r11, T hx, T hy, const T (&v)[3]) {
   if constexpr (P2Z_PACKED_F32X2 && FORM == FORM_PRECISE && std::is_same<T, float>::value) {
-    update_v2_apply_packed(s, r00, r01, r11, hx, hy);
+    update_v2_apply_packed<FIRST>(s, r00, r01, r11, hx, hy, v[0], v[1], v[2]);
     return;
   }
+  (void)v;
   const T K0 = s.c00 * r00 + s.c10 * r01, K1 = s.c00 * r01 + s.c10 * r11;
   const T K2 = s.c10 * r00 + s.c11 * r01, K3 = s.c10 * r01 + s.c11 * r11;
   const T K6 = s.c30 * r00 + s.c31 * r01, K7 = s.c30 * r01 + s.c31 * r11;
@@ -743,7 +810,7 @@ __device__ __forceinline__ void update_v2_apply(Trk<T, A> &s, T r00, T r01, T r1
 // exact determinant of the float entries, the same bound as the FP64 product
 // rounded to float) and a correctly rounded float reciprocal -- no FP64.
 // Returns true when det <= 0 (or NaN).
-template <typename A, int FORM>
+template <typename A, int FORM, bool FIRST = false>
 __device__ __forceinline__ bool update_v2(Trk<float, A> &s, const float (&hp)[3], const float (&hc)[3]) {
   float r00 = s.c00 + hc[0];
   float r01 = s.c10 + hc[1];
@@ -763,7 +830,7 @@ __device__ __forceinline__ bool update_v2(Trk<float, A> &s, const float (&hp)[3]
   r01 *= -sc;
   r11 = sc * r00;
   r00 = tmp;
-  update_v2_apply<float, A, FORM>(s, r00, r01, r11, hp[0], hp[1]);
+  update_v2_apply<float, A, FORM, FIRST>(s, r00, r01, r11, hp[0], hp[1], hc);
   return bad;
 }
 
@@ -772,7 +839,7 @@ __device__ __forceinline__ bool update_v2_f64(Trk<double, double> &s, const doub
   const double r00 = s.c00 + hc[0], r01 = s.c10 + hc[1], r11 = s.c11 + hc[2];
   const double det = r00 * r11 - r01 * r01;
   const double id = 1.0 / det;
-  update_v2_apply<double, double, FORM_PRECISE>(s, r11 * id, -r01 * id, r00 * id, hp[0], hp[1]);
+  update_v2_apply<double, double, FORM_PRECISE>(s, r11 * id, -r01 * id, r00 * id, hp[0], hp[1], hc);
   return !(det > 0.0);
 }
 

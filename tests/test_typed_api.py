@@ -1,0 +1,152 @@
+"""The reference's typed surface (include/p2z_types.hpp) and the resumable
+reference random stream behind prepareTracks / prepareHits.
+
+CPU: the stream equals the C library's rand() after srand(seed); the split
+p2z_prepare_tracks + p2z_prepare_hits equals p2z_prepare; a C++ program
+written in the shape of the reference's main compiles against the header
+(sizes defined as macros first, as the reference does) for every bsize.
+GPU: that program, driving the layer loop with propagateToZ /
+KalmanUpdate_v2, reproduces the reference's printed validation block and, bit
+for bit, the reference's own outputs built without FMA contraction."""
+import ctypes
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+SRC = ROOT / "tests" / "cpp" / "typed_main.cpp"
+PKG = ROOT / "p2z-tests_b200"
+
+
+class RefRng(ctypes.Structure):
+    _fields_ = [("ring", ctypes.c_uint32 * 31), ("have_second", ctypes.c_int32), ("next", ctypes.c_int64),
+                ("second", ctypes.c_float), ("reserved", ctypes.c_int32)]
+
+
+@pytest.mark.parametrize("seed", [1, 0, 7, 12345, 2**31 - 1, 2**32 - 5])
+def test_ref_rng_is_the_c_library_rand(p2z, seed):
+    libc = ctypes.CDLL(None)
+    libc.srand(ctypes.c_uint(seed))
+    want = [libc.rand() for _ in range(2000)]
+    g = RefRng()
+    p2z.lib.p2z_ref_rng_seed(ctypes.byref(g), seed)
+    got = [p2z.lib.p2z_ref_rng_rand(ctypes.byref(g)) for _ in range(2000)]
+    assert got == want
+    libc.srand(1)  # leave the process-wide generator as a fresh process has it
+
+
+def test_ref_rng_state_is_a_plain_copyable_struct(p2z):
+    g = RefRng()
+    p2z.lib.p2z_ref_rng_seed(ctypes.byref(g), 1)
+    for _ in range(37):
+        p2z.lib.p2z_ref_rng_randn(ctypes.byref(g))  # odd count: a cached second variate is pending
+    h = RefRng.from_buffer_copy(g)
+    a = [p2z.lib.p2z_ref_rng_randn(ctypes.byref(g)) for _ in range(50)]
+    b = [p2z.lib.p2z_ref_rng_randn(ctypes.byref(h)) for _ in range(50)]
+    assert a == b
+
+
+@pytest.mark.parametrize("bsize", [8, 32, 64])
+def test_split_prepare_equals_p2z_prepare(p2z, kat_seed, bsize):
+    trk0 = p2z.make_atrk(*kat_seed[0])
+    hits0 = p2z.make_ahits(kat_seed[1])
+    t, h = p2z.prepare(trk0, hits0, bsize, 2, 128, 20)
+    g = RefRng()
+    p2z.lib.p2z_ref_rng_seed(ctypes.byref(g), 1)
+    t2 = np.empty_like(t)
+    h2 = np.empty_like(h)
+    assert p2z.lib.p2z_prepare_tracks(ctypes.byref(g), ctypes.byref(trk0), bsize, 2, 128, 1e-7, 100.0,
+                                      t2.ctypes.data) == 0
+    assert p2z.lib.p2z_prepare_hits(ctypes.byref(g), hits0, len(kat_seed[1]), bsize, 2, 128, 20, 1e-7,
+                                    h2.ctypes.data) == 0
+    assert np.array_equal(t.view(np.uint32), t2.view(np.uint32))
+    assert np.array_equal(h.view(np.uint32), h2.view(np.uint32))
+
+
+def test_prepare_hits_rejects_too_few_seeds(p2z, kat_seed):
+    g = RefRng()
+    p2z.lib.p2z_ref_rng_seed(ctypes.byref(g), 1)
+    out = np.empty((4, 20, 9, 32), np.float32)
+    rc = p2z.lib.p2z_prepare_hits(ctypes.byref(g), p2z.make_ahits(kat_seed[1][:10]), 10, 32, 1, 128, 20, 1e-7,
+                                  out.ctypes.data)
+    assert rc == p2z.BAD_ARG
+
+
+def _compile(tmp_path, defines=()):
+    exe = tmp_path / "typed_main"
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{ROOT / 'include'}", *defines, "-o", str(exe),
+           str(SRC), f"-L{PKG}", "-lp2z", f"-Wl,-rpath,{PKG}"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+@pytest.mark.parametrize("bsize", [8, 16, 32, 64])
+def test_reference_shaped_program_compiles(tmp_path, bsize):
+    """The header takes the reference's size macros defined before it."""
+    _compile(tmp_path, (f"-Dbsize={bsize}", "-Dnevts=2", f"-Dntrks={4 * bsize}"))
+
+
+def _block(stdout):
+    vals = {}
+    for l in stdout.splitlines():
+        if l.startswith("track ") and "avg=" in l:
+            vals[l.split()[1].split("/")[0]] = float(l.split("avg=")[1].split()[0])
+    return vals
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["layers", "run"])
+def test_reference_shaped_program_prints_the_golden_block(tmp_path, oracle, mode):
+    """The known-answer input (100 x 9600, bsize 32) with the reference's
+    rounding -- layer by layer through propagateToZ / KalmanUpdate_v2, or the
+    fused pass -- prints the block of logs/propagate_gcc_omp.log:30-40 (the
+    last printed digit of pt may differ by one, as between the reference's own
+    builds), and its output array equals the reference built without FMA
+    contraction and with correctly rounded sinf/cosf, bit for bit."""
+    exe = _compile(tmp_path)
+    out = tmp_path / "out.bin"
+    r = subprocess.run([str(exe), str(GOLDEN / "kat_seed.txt"), mode, str(out)], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    gold = json.loads((GOLDEN / "kat_block.json").read_text())["blocks"]["propagate_gcc_omp.log"]
+    vals = _block(r.stdout)
+    assert r.stdout.splitlines()[-1] == "number of tracks failed=0"
+    for k in ("x", "y", "z", "dx", "dy", "pt", "phi", "theta"):
+        want = float(gold[k][0] if isinstance(gold[k], list) else gold[k])
+        assert abs(vals[k] - want) <= 1.5e-6, (k, vals[k], want)
+    if oracle.ref_available("b32_nofma_crtrig"):
+        import sys
+        sys.path.insert(0, str(ROOT / "tests"))
+        from conftest import load_p2z
+        p2z = load_p2z()
+        t, h = p2z.prepare(p2z.make_atrk(*_seed()[0]), p2z.make_ahits(_seed()[1]), 32, 100, 9600, 20)
+        ref = oracle.ref_run(t, h, nev=100, nthreads=os.cpu_count() or 1, name="b32_nofma_crtrig")
+        got = np.fromfile(out, dtype=np.float32).reshape(ref.shape)
+        assert int((got.view(np.uint32) != ref.view(np.uint32)).sum()) == 0
+
+
+@pytest.mark.gpu
+def test_reference_shaped_program_precise_block(tmp_path):
+    """The fused pass with the default (precise) evaluation prints the block of
+    the FP64 oracle (tests/golden/kat_block.json, fp64_block) within 2e-6
+    relative (the reference's own FP32 block is 1.6e-5 from it)."""
+    exe = _compile(tmp_path)
+    r = subprocess.run([str(exe), str(GOLDEN / "kat_seed.txt"), "precise"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    f = json.loads((GOLDEN / "kat_block.json").read_text())["fp64_block"]
+    vals = _block(r.stdout)
+    want = {"x": f["avgx"], "y": f["avgy"], "z": f["avgz"], "pt": f["avgpt"], "phi": f["avgphi"],
+            "theta": f["avgtheta"]}
+    for k, w in want.items():
+        assert abs(vals[k] - float(w)) <= 1.5e-6 + 2e-6 * abs(float(w)), (k, vals[k], w)
+
+
+def _seed():
+    from conftest import read_seed
+    return read_seed(GOLDEN / "kat_seed.txt")
