@@ -71,9 +71,14 @@ typedef enum p2z_status {
 } p2z_status;
 
 /* Measurement-update flavours.
- *  V2            the reference's KalmanUpdate_v2 (src/propagate-toz-test_OMP.cpp:503-620):
- *                2-D (x,y) update, FP32 with the 2x2 determinant and its reciprocal in FP64.
- *  V2_COMP       the same estimator with no FP64: compensated (FMA error-free) FP32 determinant.
+ *  V2            the reference's KalmanUpdate_v2 (src/propagate-toz-test_OMP.cpp:503-620): 2-D (x,y)
+ *                update, evaluated in FP32 with no FP64 instruction -- Kahan's compensated 2x2
+ *                determinant and a Newton-refined reciprocal, positions anchored at the last hit, and
+ *                each track's first update in the Joseph form (I-KH)C(I-KH)^T + KVK^T (later
+ *                updates: the reference's C - K H C).  With P2Z_FLAG_REFERENCE_ROUNDING: the
+ *                reference's own FP32 expressions instead, its determinant in FP64.
+ *  V2_COMP       the same estimator and evaluation with float-pair (double-float) accumulators for
+ *                x and y instead of anchored positions; no FP64 either.
  *  3X3_F64       3-D (x,y,z) update; the 3x3 residual covariance H C H^T + V is inverted and the
  *                covariance is updated in the Joseph form (I-KH)C(I-KH)^T + KVK^T, both in FP64.
  *                Basis: the reference's 3x3 KalmanUpdate (v1, :375-501), off its active path.
@@ -259,14 +264,23 @@ p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *
  * mask may have at most P2Z_NOALLOC_MAX_SLOTS track slots and
  * P2Z_NOALLOC_MAX_EVENTS events (larger runs return P2Z_BAD_ARG with a message
  * in p2z_last_error(NULL)); uniform runs and runs with a caller-provided mask
- * have no size limit.  AOSOA layout only (P2Z_UNSUPPORTED otherwise).
- * Enqueued on `stream` (a cudaStream_t; NULL is the
- * legacy default stream) on the current device; returns after enqueueing.
- * The first call on a device looks up the scratch array's device address (once
- * per device, with that device current); make that first call before any
- * stream capture.  All calls share the one scratch array and each call resets
- * what must start at zero, so calls whose work overlaps on the GPU (different
- * streams, or concurrent host threads) race on it: serialise them. */
+ * have no size limit.  AOSOA layout only (P2Z_UNSUPPORTED otherwise).  The
+ * schedule, block size 0 and the P2Z_FLAG_SORT_WINDOWS / _PER_EVENT_STREAMS
+ * flags do not apply (always the persistent pass in stored slot order, 128
+ * threads per CTA unless block_threads is set); niter passes are run.  No
+ * status comes back from the device, so P2Z_FLAG_STRICT and
+ * P2Z_FLAG_CHECK_INPUTS return P2Z_UNSUPPORTED.  For uneven events without a
+ * mask, event_ntrks is read from host memory when the call is made.
+ * Enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream:
+ * there is no context stream here) on the current device; returns after
+ * enqueueing.  The first call on a device looks up the scratch array's device
+ * address (once per device, with that device current) and keeps it for the
+ * life of the process, so a device that is reset (cudaDeviceReset) must not
+ * be used with this entry point afterwards in that process; make that first
+ * call before any stream capture.  All calls share the one scratch array and
+ * each call resets what must start at zero, so calls whose work overlaps on
+ * the GPU (different streams, or concurrent host threads) race on it:
+ * serialise them. */
 #define P2Z_NOALLOC_MAX_SLOTS (1 << 20)
 #define P2Z_NOALLOC_MAX_EVENTS (1 << 16)
 p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *d_trk_in, const void *d_hits,

@@ -16,7 +16,8 @@
 // process exits.  Host code must not use the array's name as a device
 // address: it is a host-side stand-in.  The device address is obtained once
 // per device with cudaGetSymbolAddress, with that device current, on the
-// first call on that device.
+// first call on that device, and kept for the life of the process (a device
+// reset, which reloads the library's module at a new address, makes it stale).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -141,6 +142,11 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
     return fail(P2Z_UNSUPPORTED, "P2Z_FLAG_REFERENCE_ROUNDING applies to P2Z_UPDATE_V2 only");
   if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
     return fail(P2Z_BAD_ARG, "block_threads not a multiple of 32 in 32..256");
+  // The status word lives in the shared scratch and no call returns it, so
+  // the flags that report through it are refused rather than ignored.
+  if (cfg->flags & (P2Z_FLAG_STRICT | P2Z_FLAG_CHECK_INPUTS))
+    return fail(P2Z_UNSUPPORTED, "P2Z_FLAG_STRICT and P2Z_FLAG_CHECK_INPUTS need p2z_run_device (this entry point "
+                                 "returns no status from the device)");
   // slots of the run, without allocating: sum over events of ceil(n/B)*B
   const bool uneven = cfg->event_ntrks != nullptr;
   int64_t nslots = 0;
@@ -185,8 +191,6 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const uint32_t all = cfg->nlayer >= 32 ? 0xffffffffu : ((1u << cfg->nlayer) - 1u);
-  // what must start at zero: the work counter and the status word
-  if ((e = cudaMemsetAsync(scratch, 0, 16, st)) != cudaSuccess) return fail(P2Z_CUDA_ERROR, cudaGetErrorString(e));
   if (nslots == 0) return P2Z_OK;
   const uint32_t *mask = d_hit_mask;
   if (build_mask) {
@@ -220,7 +224,12 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
   const int occ = std::max(1, kernel_occupancy(spec));
   const int64_t items = (nslots + 31) / 32;
   spec.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * nsm, (items * 32 + spec.block - 1) / spec.block));
-  if ((e = dispatch_kernel(spec, st)) != cudaSuccess) return fail(P2Z_CUDA_ERROR, cudaGetErrorString(e));
+  const int niter = cfg->niter > 0 ? cfg->niter : 1;
+  for (int it = 0; it < niter; ++it) {
+    // what must start at zero: the work counter and the status word
+    if ((e = cudaMemsetAsync(scratch, 0, 16, st)) != cudaSuccess) return fail(P2Z_CUDA_ERROR, cudaGetErrorString(e));
+    if ((e = dispatch_kernel(spec, st)) != cudaSuccess) return fail(P2Z_CUDA_ERROR, cudaGetErrorString(e));
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(P2Z_CUDA_ERROR, cudaGetErrorString(e));
   return P2Z_OK;
 }

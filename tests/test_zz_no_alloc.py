@@ -72,3 +72,51 @@ def test_noalloc_rejects_runs_beyond_its_scratch(p2z):
     assert rc == p2z.BAD_ARG
     msg = p2z.lib.p2z_last_error(None).decode()
     assert "limits are 1048576 slots" in msg
+
+
+def test_noalloc_event_limit_and_largest_event_count(p2z, ctx):
+    """P2Z_NOALLOC_MAX_EVENTS + 1 events without a mask are refused; exactly
+    P2Z_NOALLOC_MAX_EVENTS small events (some empty), which run the offsets
+    scan at its largest, give run_device's results bit for bit."""
+    import torch
+    over = np.ones(65537, dtype=np.int64)
+    cfg = p2z.make_config(bsize=8, nevts=len(over), event_ntrks=over, nlayer=20)
+    assert p2z.lib.p2z_run_device_noalloc(ctypes.byref(cfg), None, None, None, None, None) == p2z.BAD_ARG
+    assert "65536 events" in p2z.lib.p2z_last_error(None).decode()
+    rng = np.random.default_rng(5)
+    counts = rng.integers(0, 10, 65536).astype(np.int64)  # 0..9 tracks: 0, 8 or 16 slots per event
+    cfg = p2z.make_config(bsize=8, nevts=len(counts), event_ntrks=counts, nlayer=20)
+    t, h = p2z.generate_physics(cfg)
+    assert p2z.num_batches(cfg) * 8 <= 1 << 20
+    dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+    ref = torch.empty_like(dt)
+    ctx.run_device(cfg, dt, dh, ref)
+    stream = torch.cuda.Stream()
+    for _ in range(2):
+        out = torch.full_like(dt, float("nan"))
+        torch.cuda.synchronize()
+        _noalloc(p2z, cfg, dt, dh, None, out, stream)
+        stream.synchronize()
+        _compare(p2z, out.cpu().numpy(), ref.cpu().numpy())
+
+
+def test_noalloc_refuses_status_flags_and_runs_niter(p2z, ctx):
+    """No status word comes back from this entry point, so the flags that
+    report through one are refused; niter passes give the one-pass result."""
+    import torch
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=256, nlayer=20)
+    for flag in (p2z.FLAG_STRICT, p2z.FLAG_CHECK_INPUTS):
+        cfg.flags = flag
+        assert p2z.lib.p2z_run_device_noalloc(ctypes.byref(cfg), None, None, None, None, None) == p2z.UNSUPPORTED
+    cfg.flags = 0
+    t, h = p2z.generate_physics(cfg)
+    dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+    ref = torch.empty_like(dt)
+    ctx.run_device(cfg, dt, dh, ref)
+    cfg.niter = 3
+    out = torch.full_like(dt, float("nan"))
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    _noalloc(p2z, cfg, dt, dh, None, out, stream)
+    stream.synchronize()
+    _compare(p2z, out.cpu().numpy(), ref.cpu().numpy())
