@@ -396,6 +396,54 @@ def run_reference(args):
 # our arm
 # ---------------------------------------------------------------------------
 
+def reference_gpu(p2z, ctx, dt, dh, stream, launch):
+    """The reference's own GPU build (src/propagate-toz-test_CUDA_v4.cu,
+    unchanged, oracle/_ref/cuda_v4/p2z_cuda_v4_n100: 100 events x 9600 tracks
+    x 20 layers, 200 passes, its kernels on 10 streams, device-resident data)
+    run as its own process, and this library's kernel on the first 100 events
+    of the bench sample, timed the reference's way: host wall clock around the
+    200 passes and a final device synchronise."""
+    import torch
+    exe = ROOT / "oracle" / "_ref" / "cuda_v4" / "p2z_cuda_v4_n100"
+    if not exe.exists():
+        return None
+    torch.cuda.synchronize()
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    fmt = [l.split() for l in r.stdout.splitlines() if l.startswith("formatted ")]
+    if r.returncode != 0 or not fmt:
+        return {"unavailable": f"exit {r.returncode}: {r.stderr[-200:]}"}
+    niter, nev, ntrk, wall, setup = int(fmt[0][1]), int(fmt[0][2]), int(fmt[0][3]), float(fmt[0][6]), float(fmt[0][8])
+    upd = nev * ntrk * 20
+    cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=ntrk, nlayer=20, schedule=launch["schedule"],
+                          block_threads=launch["block_threads"])
+    nb = nev * ntrk // 32
+    t, h = dt[:nb], dh[:nb]
+    o = torch.empty_like(t)
+    args = (ctx.h, p2z.C.byref(cfg), t.data_ptr(), h.data_ptr(), None, o.data_ptr(),
+            p2z.C.c_void_p(stream.cuda_stream), None)
+    for _ in range(3):
+        p2z.lib.p2z_run_device(*args)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(niter):
+        p2z.lib.p2z_run_device(*args)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ours_wall = time.perf_counter() - t0
+    ours_dev = e0.elapsed_time(e1) / 1e3
+    return {"binary": "oracle/_ref/cuda_v4/p2z_cuda_v4_n100: src/propagate-toz-test_CUDA_v4.cu unchanged, its "
+                      "Makefile's nvcc flags (MODE=cudav4, USE_ASYNC) for sm_100a, -Dnevts=100 -DNITER=200",
+            "workload": f"{nev} events x {ntrk} tracks x 20 layers, {niter} passes, device-resident (its own "
+                        "smeared known-answer input; this library: the first 100 events of the bench sample)",
+            "reference_updates_per_s": upd * niter / wall, "reference_ms_per_pass": 1e3 * wall / niter,
+            "reference_setup_s": setup,
+            "ours_updates_per_s_wall": upd * niter / ours_wall, "ours_ms_per_pass_wall": 1e3 * ours_wall / niter,
+            "ours_updates_per_s_device": upd * niter / ours_dev,
+            "ratio_wall": wall / ours_wall}
+
+
 def cpu_model():
     """The host CPU's model name (as lscpu reports it), or None."""
     try:
@@ -451,6 +499,8 @@ def main():
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip running the reference's own CUDA_v4 build beside this kernel")
     ap.add_argument("--serve-events", type=int, default=1500)
     ap.add_argument("--serve-inflight", type=int, default=8, help="server groups in flight (1..8)")
     ap.add_argument("--serve-rates", default="", help="comma-separated offered rates (events/s); default sweep")
@@ -532,6 +582,13 @@ def main():
     value = updates * world / (ms_step / 1e3)
     st = ctx.run_device(cfg, dt, dh, do)  # one more pass for the launch count and status
     launches_per_step = st.launches
+    launch = {"schedule": (args.schedule if args.schedule != "auto" else
+                           (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
+              "block_threads": (args.block or (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head
+                                               else 128))}
+    ref_gpu = None
+    if rank == 0 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu(p2z, ctx, dt, dh, stream, launch)
 
     # e2e: host buffers through p2z_run
     e2e = None
@@ -697,10 +754,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(nev, world),
         "form": "precise (default; no FP64 instruction)",
-        "launch": {"schedule": (args.schedule if args.schedule != "auto" else
-                                (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
-                   "block_threads": (args.block or
-                                     (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head else 128))},
+        "launch": launch,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": (tpu * updates / launches_per_step) if tpu else None,
@@ -724,6 +778,7 @@ def main():
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,
         "batched_vs_plain": bvp,
+        "reference_gpu": ref_gpu,
         "serving": serving,
         "outputs_finite": out_ok,
     }

@@ -375,6 +375,23 @@ p2z_status p2z_prepare_tracks(p2z_ref_rng *g, const p2z_atrk *seed, int bsize, i
 p2z_status p2z_prepare_hits(p2z_ref_rng *g, const p2z_ahit *hit_seeds, int nseeds, int bsize, int64_t nevts,
                             int64_t ntrks, int nlayer, double smear, void *hits_out);
 
+/* p2z_prepare generated on the device into device buffers (AOSOA, bsize
+ * batches): the same words as p2z_prepare, for callers whose tracks and hits
+ * live on the GPU.  The reference's rand() stream is split into chunks whose
+ * starting states are computed by jumping its additive generator ahead, the
+ * polar method's accepted attempts are counted per chunk and prefix-summed,
+ * and every variate is written to its word in parallel.  The variate's log is
+ * correctly rounded where p2z_prepare calls the C library's logf (which
+ * differs in the last place for ~0.3% of variates; that changed no output
+ * word on 200M variates, and the tests compare the outputs word for word).
+ * Scratch from the context.  Enqueued on `stream` (NULL = the context's
+ * stream); returns when the output is complete.  No counterpart in the
+ * reference, which prepares on the host (src/propagate-toz-test_OMP.cpp:
+ * 243-293). */
+p2z_status p2z_prepare_device(p2z_context *ctx, const p2z_atrk *seed, const p2z_ahit *hit_seeds, int nseeds,
+                              int bsize, int64_t nevts, int64_t ntrks, int nlayer, double smear, double cov_scale,
+                              void *d_trk_out, void *d_hits_out, void *stream);
+
 /* Physics workload generator (no counterpart in the reference): tracks of
  * charge +-1, pT log-uniform in [pt_min, pt_max] GeV, phi ~ U(-pi, pi),
  * eta ~ U(eta_min, eta_max), vertex z ~ N(0, sigma_vz); covariance

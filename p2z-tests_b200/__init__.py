@@ -173,6 +173,8 @@ _SIGS = {
                                   C.c_float]),
     "p2z_prepare": (C.c_int, [C.POINTER(Atrk), C.POINTER(Ahit), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int,
                               C.c_double, C.c_double, _VP, _VP]),
+    "p2z_prepare_device": (C.c_int, [_VP, C.POINTER(Atrk), C.POINTER(Ahit), C.c_int, C.c_int, C.c_int64, C.c_int64,
+                                     C.c_int, C.c_double, C.c_double, _VP, _VP, _VP]),
     "p2z_physics_defaults": (None, [C.POINTER(PhysicsParams)]),
     "p2z_generate_physics": (C.c_int, [C.POINTER(PhysicsParams), C.POINTER(Config), _VP, _VP, _VP]),
     "p2z_mask_layers": (C.c_int, [_VP, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64]),
@@ -571,6 +573,13 @@ class Context:
         _wait_for_torch(d_trk, d_hits)
         _check(lib.p2z_step_device(self.h, bsize, nbatches, _ptr(d_trk), _ptr(d_hits), nlayer, layer, what, update,
                                    kfact), self.h)
+
+    def prepare_device(self, seed: Atrk, hit_seeds, bsize, nevts, ntrks, nlayer, d_trk, d_hits, smear=1e-7,
+                       cov_scale=100.0, stream=None):
+        """p2z_prepare on the device (p2z_prepare_device), into device buffers."""
+        stream = _stream(stream, d_trk, d_hits)
+        _check(lib.p2z_prepare_device(self.h, C.byref(seed), hit_seeds, len(hit_seeds), bsize, nevts, ntrks, nlayer,
+                                      smear, cov_scale, _ptr(d_trk), _ptr(d_hits), stream), self.h)
 
     def generate_physics_device(self, cfg: Config, d_trk, d_hits, d_mask=None, params=None, stream=None):
         """The physics sample generated on the device (p2z_generate_physics_device)."""

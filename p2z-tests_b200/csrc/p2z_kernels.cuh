@@ -75,7 +75,7 @@ struct RunArgs {
   unsigned int *status;            // bit 0: a det <= 0 was met; bit 1: a staging wait timed out
   unsigned long long *queue;       // persistent kernels: next work item
   int64_t ws;                      // SoA layout (B == 0): slots in the arrays = word stride
-  // Sorted windows (masked runs): the launch's slots are split into windows
+  // Sorted windows (masked kernels only): the launch's slots are split into windows
   // of `win` slots from slot_begin; the thread at linear slot s processes
   // slot window_base(s) + perm[s].  perm == nullptr: s itself.
   const uint8_t *__restrict__ perm;
@@ -304,7 +304,7 @@ template <int B, int UPD, int SC, bool MASKED>
 __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_flat(RunArgs a) {
   const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= a.slot_end) return;
-  process_slot<B, UPD, SC, MASKED>(a, map_slot(a, slot));
+  process_slot<B, UPD, SC, MASKED>(a, MASKED ? map_slot(a, slot) : slot);
 }
 
 // Persistent launch: grid = resident CTAs; each warp repeatedly takes the next
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArg
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nitems) break;
     const int64_t slot = a.slot_begin + (int64_t)item * 32 + lane;
-    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, map_slot(a, slot));
+    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, MASKED ? map_slot(a, slot) : slot);
   }
 }
 

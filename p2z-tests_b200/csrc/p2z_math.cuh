@@ -638,33 +638,39 @@ __device__ __forceinline__ float det2_comp(float a, float b, float c, float d) {
 // relative error grows with R's condition number) costs many digits: on a
 // track whose first hit is 200x more precise than the track in one
 // direction, C then stops describing the track, and the gains of later
-// layers with it.  That is the first update of a track, where its prior
-// covariance meets a measurement, so a track's first update (FIRST) takes the
-// Joseph form (I-KH) C (I-KH)^T + K V K^T instead, evaluated as
-// C'' = P - E K^T with P = C - K H C and E = P H^T - K V, the residual of the
-// gain equation, which cancels K's rounding errors to first order.  K V is
-// formed from error-free products (p = K0*v, e = fma(K0, v, -p)): with an
-// elongated V (eigenvalues 1e6 apart on the reference's known-answer hits)
-// the two products cancel, and a rounded first product would leave an error
-// of eps*|K||V| in E.  Later updates keep C - K H C: after the first update C
-// is already a fit of the track and an update shrinks it by small factors,
-// where C - K H C is accurate, at 22 instructions against the Joseph form's
-// 69.  Measured on one B200: Joseph on every layer costs 10.8% of the pass,
-// with the same results on every sample tried (single-seed, known-answer,
-// physics and the conditioning sweep); choosing per track by the shrink
-// det(I - K H) costs more than Joseph on every first layer, because physics
-// tracks straddle any threshold and a warp then runs both forms.
-template <bool FIRST, typename A>
-__device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float i00, float i01, float i11, float hx,
+// layers with it.  That happens at a track's first update, where its prior
+// covariance meets a measurement.  There, when g = det(V)/det(R) =
+// det(I - K H) is at or below kJosephShrink (a shrink of 100 or more in area),
+// the update takes the Joseph form (I-KH) C (I-KH)^T + K V K^T instead,
+// evaluated as C'' = P - E K^T with P = C - K H C and E = P H^T - K V, the
+// residual of the gain equation, which cancels K's rounding errors to first
+// order.  K V is formed from error-free products (p = K0*v, e = fma(K0, v,
+// -p)): with an elongated V the two products cancel, and a rounded first
+// product would leave an error of eps*|K||V| in E.  The reference's own
+// known-answer hits are such a V (eigenvalues 1e6 apart) and their first
+// updates shrink little in area (g > 0.01); there C - K H C is the more
+// accurate evaluation (1e-4 against the Joseph form's 7.5e-4 in q/pT), as it
+// is everywhere after a track's first update, where C is already a fit of
+// the track.  The test is per track, so a track's result does not depend on
+// its neighbours.  Measured on one B200 (1000 x 9600 physics sample, flat
+// launch; without the first-layer test 1.770 ms): the test 1.786 ms, the
+// Joseph form on every first layer unconditionally 1.841 ms, on every layer
+// 1.961 ms, with the same results on the single-seed, physics and sweep
+// samples.
+constexpr float kJosephShrink = 0.01f;
+
+// Joseph form of a track's first update (see above).
+template <typename A>
+__device__ __forceinline__ void update_v2_apply_joseph(Trk<float, A> &s, float i00, float i01, float i11, float hx,
                                                        float hy, float v00, float v01, float v11) {
   const float2 I0 = make_float2(i00, i01), I1 = make_float2(i01, i11);
   const float2 A0 = make_float2(s.c00, s.c10), A1 = make_float2(s.c10, s.c11);
   const float2 B3 = make_float2(s.c30, s.c31), B4 = make_float2(s.c40, s.c41), B5 = make_float2(s.c50, s.c51);
   const float2 Kx = fma2(bc2(s.c10), I1, mul2(bc2(s.c00), I0));  // (K0, K1)
   const float2 Ky = fma2(bc2(s.c11), I1, mul2(bc2(s.c10), I0));  // (K2, K3)
-  const float2 Ki = fma2(bc2(B3.y), I1, mul2(bc2(B3.x), I0));  // (K6, K7)
-  const float2 Kp = fma2(bc2(B4.y), I1, mul2(bc2(B4.x), I0));  // (K8, K9)
-  const float2 Kt = fma2(bc2(B5.y), I1, mul2(bc2(B5.x), I0));  // (K10, K11)
+  const float2 Ki = fma2(bc2(B3.y), I1, mul2(bc2(B3.x), I0));    // (K6, K7)
+  const float2 Kp = fma2(bc2(B4.y), I1, mul2(bc2(B4.x), I0));    // (K8, K9)
+  const float2 Kt = fma2(bc2(B5.y), I1, mul2(bc2(B5.x), I0));    // (K10, K11)
   const float res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
   acc_update(s.x, hx, res0, Kx.x * res0 + Kx.y * res1);
   acc_update(s.y, hy, res1, Ky.x * res0 + Ky.y * res1);
@@ -680,21 +686,7 @@ __device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float i
   const float2 Pi = fma2(bc2(-Ki.y), A1, fma2(bc2(-Ki.x), A0, B3));
   const float2 Pp = fma2(bc2(-Kp.y), A1, fma2(bc2(-Kp.x), A0, B4));
   const float2 Pt = fma2(bc2(-Kt.y), A1, fma2(bc2(-Kt.x), A0, B5));
-  if constexpr (!FIRST) {
-    s.c00 = Px.x;
-    s.c10 = Py.x; s.c11 = Py.y;
-    s.c30 = Pi.x; s.c31 = Pi.y;
-    s.c40 = Pp.x; s.c41 = Pp.y;
-    s.c50 = Pt.x; s.c51 = Pt.y;
-    s.c33 = fmaf(-Ki.y, B3.y, fmaf(-Ki.x, B3.x, s.c33));
-    s.c43 = fmaf(-Kp.y, B3.y, fmaf(-Kp.x, B3.x, s.c43));
-    s.c44 = fmaf(-Kp.y, B4.y, fmaf(-Kp.x, B4.x, s.c44));
-    s.c53 = fmaf(-Kt.y, B3.y, fmaf(-Kt.x, B3.x, s.c53));
-    s.c54 = fmaf(-Kt.y, B4.y, fmaf(-Kt.x, B4.x, s.c54));
-    s.c55 = fmaf(-Kt.y, B5.y, fmaf(-Kt.x, B5.x, s.c55));
-    return;
-  }
-  // Joseph form: E_i = P_i - K_i V (K V from error-free products), then
+  // E_i = P_i - K_i V (K V from error-free products), then
   // C''(i, m) = P(i, m) - E_i . K_m for the measured columns and
   // C''(a, b) = C(a, b) - K_a . B_b - E_a . K_b on the unmeasured block.
   const float2 V0 = make_float2(v00, v01), V1 = make_float2(v01, v11);
@@ -721,6 +713,57 @@ __device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float i
   s.c30 = Ni.x; s.c31 = Ni.y;
   s.c40 = Np.x; s.c41 = Np.y;
   s.c50 = Nt.x; s.c51 = Nt.y;
+}
+
+// Every later update: the reference's C - K H C with the column-0/1 pairs of
+// rows y, ipt, phi, theta updated together:
+//   (c_i0, c_i1)' = (c_i0, c_i1) - K_i0 (c00, c10) - K_i1 (c10, c11).
+template <bool FIRST, typename A>
+__device__ __forceinline__ void update_v2_apply_packed(Trk<float, A> &s, float r00, float r01, float r11, float hx,
+                                                       float hy, float v00, float v01, float v11) {
+  if constexpr (FIRST) {
+    // shrink test: det(I - K H) = det(V) / det(R), and r00 r11 - r01^2 = 1/det(R)
+    const float g = fmaf(v00, v11, -(v01 * v01)) * fmaf(r00, r11, -(r01 * r01));
+    if (!(g > kJosephShrink)) {
+      update_v2_apply_joseph(s, r00, r01, r11, hx, hy, v00, v01, v11);
+      return;
+    }
+  }
+  (void)v00;
+  (void)v01;
+  (void)v11;
+  const float2 R0 = make_float2(r00, r01), R1 = make_float2(r01, r11);
+  const float2 Kx = fma2(bc2(s.c10), R1, mul2(bc2(s.c00), R0));  // (K0, K1)
+  const float2 Ky = fma2(bc2(s.c11), R1, mul2(bc2(s.c10), R0));  // (K2, K3)
+  const float2 Ki = fma2(bc2(s.c31), R1, mul2(bc2(s.c30), R0));  // (K6, K7)
+  const float2 Kp = fma2(bc2(s.c41), R1, mul2(bc2(s.c40), R0));  // (K8, K9)
+  const float2 Kt = fma2(bc2(s.c51), R1, mul2(bc2(s.c50), R0));  // (K10, K11)
+  const float res0 = acc_res(hx, s.x), res1 = acc_res(hy, s.y);
+  acc_update(s.x, hx, res0, Kx.x * res0 + Kx.y * res1);
+  acc_update(s.y, hy, res1, Ky.x * res0 + Ky.y * res1);
+  const float dphi = Kp.x * res0 + Kp.y * res1;
+  const float dth = Kt.x * res0 + Kt.y * res1;
+  acc_add(s.phi, dphi);
+  s.theta = __fadd_rn(s.theta, dth);
+  turn_direction(s, dphi, dth);
+  s.ipt = s.ipt + Ki.x * res0 + Ki.y * res1;
+  const float2 P0 = make_float2(s.c00, s.c10), Q = make_float2(s.c10, s.c11);
+  const float c30 = s.c30, c31 = s.c31, c40 = s.c40, c41 = s.c41, c50 = s.c50, c51 = s.c51;
+  s.c00 = fmaf(-Kx.y, s.c10, fmaf(-Kx.x, s.c00, s.c00));
+  const float2 Ny = fma2(bc2(-Ky.y), Q, fma2(bc2(-Ky.x), P0, Q));
+  const float2 Ni = fma2(bc2(-Ki.y), Q, fma2(bc2(-Ki.x), P0, make_float2(c30, c31)));
+  const float2 Np = fma2(bc2(-Kp.y), Q, fma2(bc2(-Kp.x), P0, make_float2(c40, c41)));
+  const float2 Nt = fma2(bc2(-Kt.y), Q, fma2(bc2(-Kt.x), P0, make_float2(c50, c51)));
+  s.c10 = Ny.x; s.c11 = Ny.y;
+  s.c30 = Ni.x; s.c31 = Ni.y;
+  s.c40 = Np.x; s.c41 = Np.y;
+  s.c50 = Nt.x; s.c51 = Nt.y;
+  s.c33 = fmaf(-Ki.y, c31, fmaf(-Ki.x, c30, s.c33));
+  s.c43 = fmaf(-Kp.y, c31, fmaf(-Kp.x, c30, s.c43));
+  s.c44 = fmaf(-Kp.y, c41, fmaf(-Kp.x, c40, s.c44));
+  s.c53 = fmaf(-Kt.y, c31, fmaf(-Kt.x, c30, s.c53));
+  s.c54 = fmaf(-Kt.y, c41, fmaf(-Kt.x, c40, s.c54));
+  s.c55 = fmaf(-Kt.y, c51, fmaf(-Kt.x, c50, s.c55));
 }
 
 // The generic form (FP64 kernel, reference rounding, unpacked FP32): the

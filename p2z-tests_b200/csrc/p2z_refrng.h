@@ -18,12 +18,18 @@
 
 #include "p2z.h"
 
+#if defined(__CUDACC__)
+#define P2Z_RNG_HD __host__ __device__ __forceinline__
+#else
+#define P2Z_RNG_HD inline
+#endif
+
 namespace p2z_refrng {
 
 constexpr int kLag = 31;      // long lag
 constexpr int kShort = 3;     // short lag
 constexpr int kDiscard = 344; // index of the first output's word
-constexpr float kRandMax = 2147483647.f;
+constexpr float kRandMax = 2147483647.f;  // RAND_MAX as a float: 2^31
 
 // State: ring[i % 31] holds r[i] for the 31 most recent words; `next` is the
 // index of the word the next draw produces.
@@ -55,8 +61,9 @@ inline int32_t draw(p2z_ref_rng *g) {
 
 // One attempt of the polar method on two draws, with the reference's types:
 // U = -1 + ((float)rand()/RAND_MAX)*2 in float, W = pow(U1,2) + pow(U2,2) in
-// double stored to float.  Returns W (accepted when 0 < W < 1).
-inline float attempt(int32_t d1, int32_t d2, float *u1, float *u2) {
+// double stored to float.  Returns W (accepted when 0 < W < 1).  Shared by
+// the host stream and the device generator (p2z_prep.cu).
+P2Z_RNG_HD float attempt(int32_t d1, int32_t d2, float *u1, float *u2) {
   *u1 = -1 + ((float)d1 / kRandMax) * 2;
   *u2 = -1 + ((float)d2 / kRandMax) * 2;
   return (float)((double)*u1 * (double)*u1 + (double)*u2 * (double)*u2);

@@ -65,3 +65,43 @@ def test_pass_on_device_generated_input(p2z, ctx):
     a = p2z.tracks_to_aos(out_dev.cpu().numpy().reshape(t.shape))
     b = p2z.tracks_to_aos(out_host.cpu().numpy().reshape(t.shape))
     assert par_rel(a["par"], b["par"]).max() <= 1e-5
+
+
+def _prepare_both(p2z, ctx, seed, bsize, nevts, ntrks, smear=1e-7, cov_scale=100.0):
+    import time
+    import torch
+    trk0, hits0 = p2z.make_atrk(*seed[0]), p2z.make_ahits(seed[1])
+    t0 = time.perf_counter()
+    t, h = p2z.prepare(trk0, hits0, bsize, nevts, ntrks, 20, smear=smear, cov_scale=cov_scale)
+    host_s = time.perf_counter() - t0
+    dt = torch.full((t.size,), float("nan")).cuda()
+    dh = torch.full((h.size,), float("nan")).cuda()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.prepare_device(trk0, hits0, bsize, nevts, ntrks, 20, dt, dh, smear=smear, cov_scale=cov_scale)
+    torch.cuda.synchronize()
+    dev_s = time.perf_counter() - t0
+    return t, h, dt.cpu().numpy().reshape(t.shape), dh.cpu().numpy().reshape(h.shape), host_s, dev_s
+
+
+@pytest.mark.parametrize("bsize", [8, 16, 32, 64])
+def test_prepare_device_equals_prepare(p2z, ctx, kat_seed, bsize):
+    """The reference's prepareTracks / prepareHits on the device: the words of
+    p2z_prepare (itself bit-exact with the reference's own functions)."""
+    t, h, gt, gh, _, _ = _prepare_both(p2z, ctx, kat_seed, bsize, 2, 128)
+    assert np.array_equal(t.view(np.uint32), gt.view(np.uint32))
+    assert np.array_equal(h.view(np.uint32), gh.view(np.uint32))
+
+
+@pytest.mark.parametrize("case", ["known_answer", "single_seed"])
+def test_prepare_device_full_size(p2z, ctx, kat_seed, readme_seed, case):
+    """The known-answer workload (100 x 9600, smear 1e-7, covariances x100)
+    and the single-seed one (10 x 9600, smear 1e-5, covariances as given),
+    word for word, with the host and device setup times printed."""
+    if case == "known_answer":
+        t, h, gt, gh, hs, ds = _prepare_both(p2z, ctx, kat_seed, 32, 100, 9600)
+    else:
+        t, h, gt, gh, hs, ds = _prepare_both(p2z, ctx, readme_seed, 32, 10, 9600, smear=1e-5, cov_scale=1.0)
+    print(f"{case}: host p2z_prepare {hs:.3f} s, p2z_prepare_device {ds:.4f} s ({hs / ds:.0f}x)")
+    assert int((t.view(np.uint32) != gt.view(np.uint32)).sum()) == 0
+    assert int((h.view(np.uint32) != gh.view(np.uint32)).sum()) == 0

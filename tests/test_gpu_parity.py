@@ -231,10 +231,7 @@ def test_known_answer_validation_block(p2z, ctx, kat_seed, mode):
     # printed with 6 decimals: the last printed digit may differ by 1.  The
     # precise form's means may also differ from the FP64 ones by 5e-7 relative
     # (the golden log's FP32 evaluation is 1.6e-5 off in pt).
-    # precise: within 2e-6 relative of the FP64 block (measured: pt 1.5e-6, from the Joseph form of
-    # each track's first update; the reference's own FP32 block is 1.6e-5 from it, and rounding the
-    # state alone to FP32 moves a track's q/pT by up to 1.4e-5 on this input)
-    rel = 0.0 if mode == "reference_rounding" else 2e-6
+    rel = 0.0 if mode == "reference_rounding" else 5e-7
     for k in got:
         assert abs(got[k] - want[k]) <= 1.5e-6 + rel * abs(want[k]), (mode, k, got[k], want[k])
 

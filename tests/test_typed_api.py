@@ -133,7 +133,7 @@ def test_reference_shaped_program_prints_the_golden_block(tmp_path, oracle, mode
 @pytest.mark.gpu
 def test_reference_shaped_program_precise_block(tmp_path):
     """The fused pass with the default (precise) evaluation prints the block of
-    the FP64 oracle (tests/golden/kat_block.json, fp64_block) within 2e-6
+    the FP64 oracle (tests/golden/kat_block.json, fp64_block) within 5e-7
     relative (the reference's own FP32 block is 1.6e-5 from it)."""
     exe = _compile(tmp_path)
     r = subprocess.run([str(exe), str(GOLDEN / "kat_seed.txt"), "precise"], capture_output=True, text=True,
@@ -144,7 +144,7 @@ def test_reference_shaped_program_precise_block(tmp_path):
     want = {"x": f["avgx"], "y": f["avgy"], "z": f["avgz"], "pt": f["avgpt"], "phi": f["avgphi"],
             "theta": f["avgtheta"]}
     for k, w in want.items():
-        assert abs(vals[k] - float(w)) <= 1.5e-6 + 2e-6 * abs(float(w)), (k, vals[k], w)
+        assert abs(vals[k] - float(w)) <= 1.5e-6 + 5e-7 * abs(float(w)), (k, vals[k], w)
 
 
 def _seed():
