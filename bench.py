@@ -15,10 +15,14 @@ tracks x 20 layers.  Inputs (8.1 GB) are larger than L2, so no flush is needed.
           5-20 hits per track with 10% of layers dropped): the persistent
           work-queue kernel replayed as a CUDA graph vs one launch per event,
           each with the block size the autotuner measured best for it
-  autotune  p2z_autotune's sweep (bsize x AOSOA/SoA x schedule x block size)
-          on the headline and the uneven workloads; the headline step runs
-          the reference's layout (bsize 32 AOSOA) with the schedule and block
-          size the sweep found best for that layout
+  autotune  p2z_autotune's sweep (bsize x AOSOA/SoA x schedule x block size x
+          threads per track) on the headline and the uneven workloads; the
+          headline step runs the reference's layout (bsize 32 AOSOA) with the
+          schedule, block size and threads per track the sweep found best for
+          that layout
+  threads_per_track  one against two threads per track: headline
+          throughput, and the device time of one launch over a lone event of
+          1024, 3072 or 9600 tracks
 
 `--impl reference` times the reference's own CPU hot loop (its OpenMP source
 compiled unchanged into oracle/_ref) on this host's cores, on the same
@@ -281,12 +285,86 @@ def tune_summary(best, rows, wall_s):
         return min(sel, key=lambda r: r["ms"]) if sel else None
     out = {"configurations": len(rows), "sweep_wall_s": wall_s, "best": best,
            "best_bsize32_aosoa": fastest(lambda r: r["bsize"] == 32 and r["layout"] == "aosoa")}
-    for key in ("bsize", "layout", "schedule"):
+    for key in ("bsize", "layout", "schedule", "threads_per_track"):
         vals = sorted({r[key] for r in rows}, key=str)
         out[f"best_per_{key}"] = {str(v): {"ms": fastest(lambda r: r[key] == v)["ms"],
                                            "updates_per_s": fastest(lambda r: r[key] == v)["updates_per_s"]}
                                   for v in vals}
     return out
+
+
+def threads_per_track_report(p2z, ctx, torch, dt, dh, do, stream):
+    """One thread per track against two (p2z_config.threads_per_track), flat
+    launches of the precise form at bsize 32 AOSOA: (1) throughput on the
+    headline sample, best block size each; (2) the device time of one launch
+    over a lone event of 1024, 3072 or 9600 tracks (the first batches of the
+    sample), where the GPU is mostly empty and a track's 20-layer chain sets
+    the time.  The lone-event time is the mean over 200 launches queued back
+    to back on one stream behind a sleep kernel (so that host submission does
+    not enter the timed span), between one pair of CUDA events: the kernel's
+    duration plus the gap between consecutive kernels.  (Events around each
+    launch would read in steps of the timer's 2.048 us resolution.)"""
+    def launcher(cfg, t, h, o):
+        args = (ctx.h, p2z.C.byref(cfg), t.data_ptr(), h.data_ptr(), None, o.data_ptr(),
+                p2z.C.c_void_p(stream.cuda_stream), None)
+        def go():
+            rc = p2z.lib.p2z_run_device(*args)
+            if rc != p2z.OK:
+                raise p2z.P2zError(rc, p2z.lib.p2z_last_error(ctx.h).decode())
+        return go
+
+    nev = dt.shape[0] * 32 // 9600
+    head = {}
+    for tpt in (1, 2):
+        best = None
+        for block in (32, 64, 128, 256):
+            cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule="flat", block_threads=block,
+                                  threads_per_track=tpt)
+            go = launcher(cfg, dt, dh, do)
+            for _ in range(2):
+                go()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(5):
+                go()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / 5
+            if best is None or ms < best["ms"]:
+                best = {"ms": ms, "block_threads": block, "updates_per_s": nev * 9600 * 20 / (ms / 1e3)}
+        head[str(tpt)] = best
+    lone = {}
+    for n in (1024, 3072, 9600):
+        nb = n // 32
+        row = {}
+        for tpt in (1, 2):
+            best = None
+            for block in (32, 64, 128):
+                cfg = p2z.make_config(bsize=32, nevts=1, ntrks=n, nlayer=20, schedule="flat", block_threads=block,
+                                      threads_per_track=tpt)
+                go = launcher(cfg, dt[:nb], dh[:nb], do[:nb])
+                for _ in range(3):
+                    go()
+                reps = 200
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                with torch.cuda.stream(stream):
+                    torch.cuda._sleep(40_000_000)  # ~20 ms: the queue fills while the GPU waits
+                a.record(stream)
+                for _ in range(reps):
+                    go()
+                b.record(stream)
+                torch.cuda.synchronize()
+                us = a.elapsed_time(b) * 1e3 / reps
+                if best is None or us < best["us"]:
+                    best = {"us": us, "block_threads": block}
+            row[str(tpt)] = best
+        row["ratio_1_over_2"] = row["1"]["us"] / row["2"]["us"]
+        lone[str(n)] = row
+    return {"note": "flat launches, precise form, bsize 32 AOSOA; two threads per track: lanes 2i and 2i+1 "
+                    "hold the same track and split the propagation of its covariance (bit-identical results)",
+            "headline": head, "headline_ratio_1_over_2": head["1"]["updates_per_s"] / head["2"]["updates_per_s"],
+            "lone_event_launch_us": lone}
 
 
 def run_serving(p2z, device, rank, args):
@@ -505,6 +583,7 @@ def main():
     ap.add_argument("--serve-inflight", type=int, default=8, help="server groups in flight (1..8)")
     ap.add_argument("--serve-rates", default="", help="comma-separated offered rates (events/s); default sweep")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-lanes", action="store_true", help="skip the threads-per-track comparison")
     ap.add_argument("--schedule", default="auto", choices=["auto", "flat", "persistent", "per_event", "staged"],
                     help="launch schedule of the headline step (auto: what the autotuner measured best)")
     ap.add_argument("--block", type=int, default=0, help="threads per CTA of the headline step (0: tuned)")
@@ -585,10 +664,14 @@ def main():
     launch = {"schedule": (args.schedule if args.schedule != "auto" else
                            (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
               "block_threads": (args.block or (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head
-                                               else 128))}
+                                               else 128)),
+              "threads_per_track": tune_head["best_bsize32_aosoa"]["threads_per_track"] if tune_head else 1}
     ref_gpu = None
     if rank == 0 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(p2z, ctx, dt, dh, stream, launch)
+    lanes = None
+    if rank == 0 and not args.no_lanes:
+        lanes = threads_per_track_report(p2z, ctx, torch, dt, dh, do, stream)
 
     # e2e: host buffers through p2z_run
     e2e = None
@@ -775,6 +858,7 @@ def main():
         "clocks": clk,
         "measured_peaks": live_peaks,
         "autotune": tune_head,
+        "threads_per_track": lanes,
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,
         "batched_vs_plain": bvp,

@@ -50,7 +50,7 @@
 extern "C" {
 #endif
 
-#define P2Z_ABI_VERSION 1
+#define P2Z_ABI_VERSION 2
 
 /* Field constant of the reference's OMP/TBB/CUDA_v4 family:
  * kfact = 100/(-0.299792458*3.8112) (src/propagate-toz-test_OMP.cpp:622),
@@ -173,6 +173,14 @@ typedef struct p2z_config {
   int32_t layout;        /* p2z_layout of the track, hit and output arrays */
   /* Uneven form (optional, host memory): nevts track counts.  NULL -> uniform. */
   const int64_t *event_ntrks;
+  int32_t threads_per_track; /* 1, or 2 (P2Z_UPDATE_V2 without REFERENCE_ROUNDING; FLAT,
+                            PER_EVENT and PERSISTENT schedules): lanes 2i and 2i+1 of a warp
+                            hold the same track and split the propagation of its covariance,
+                            with bit-identical results.  0 -> the value p2z_autotune measured
+                            best on this context for the same update, flags, bsize, layout
+                            and masking, else 1.  No counterpart in the reference (one thread
+                            per track in every GPU version, src/propagate-toz-test_CUDA_v4.cu:
+                            761-775) */
 } p2z_config;
 
 /* Filled by the run entry points (optional out-parameter). */
@@ -265,9 +273,10 @@ p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *
  * P2Z_NOALLOC_MAX_EVENTS events (larger runs return P2Z_BAD_ARG with a message
  * in p2z_last_error(NULL)); uniform runs and runs with a caller-provided mask
  * have no size limit.  AOSOA layout only (P2Z_UNSUPPORTED otherwise).  The
- * schedule, block size 0 and the P2Z_FLAG_SORT_WINDOWS / _PER_EVENT_STREAMS
- * flags do not apply (always the persistent pass in stored slot order, 128
- * threads per CTA unless block_threads is set); niter passes are run.  No
+ * schedule, block size 0, threads_per_track and the P2Z_FLAG_SORT_WINDOWS /
+ * _PER_EVENT_STREAMS flags do not apply (always the persistent pass in stored
+ * slot order, one thread per track, 128 threads per CTA unless block_threads
+ * is set); niter passes are run.  No
  * status comes back from the device, so P2Z_FLAG_STRICT and
  * P2Z_FLAG_CHECK_INPUTS return P2Z_UNSUPPORTED.  For uneven events without a
  * mask, event_ntrks is read from host memory when the call is made.
@@ -305,6 +314,7 @@ typedef struct p2z_tune_entry {
   int32_t layout;         /* p2z_layout */
   int32_t schedule;       /* P2Z_SCHED_FLAT, _PER_EVENT, _PERSISTENT or _STAGED */
   int32_t block_threads;  /* 32 .. 256 */
+  int32_t threads_per_track; /* 1 or 2 */
   double ms;              /* mean device time of one pass */
   double updates_per_s;   /* present-hit updates per second */
 } p2z_tune_entry;
@@ -313,7 +323,8 @@ typedef struct p2z_tune_entry {
  * iteration) on the caller's device data under every combination of bsize
  * {8,16,32,64} x layout {AOSOA, SOA} x schedule {FLAT, PERSISTENT, PER_EVENT
  * when nevts <= 4096, and STAGED at bsize 32 AOSOA} x block_threads
- * {32,64,128,256}, each the mean
+ * {32,64,128,256} x threads_per_track {1, and 2 where the update kind and
+ * schedule have it}, each the mean
  * of `reps` passes (0 -> 3) after one warm-up pass.  The inputs are converted
  * to each candidate's bsize and layout with p2z_relayout_device into scratch
  * buffers the call allocates and frees (about twice the input size); the
@@ -321,9 +332,9 @@ typedef struct p2z_tune_entry {
  * measured in *n_entries, the first max_entries of them in `entries` (may be
  * NULL when max_entries is 0), the fastest in *best.
  * Side effect: for every (bsize, layout) measured, the context remembers the
- * fastest schedule and block size, and later runs with block_threads = 0 or
- * schedule = AUTO and the same update, flags, bsize, layout and masking use
- * them.  A different bsize or layout is a different data layout, which only
+ * fastest schedule, block size and threads per track, and later runs with
+ * block_threads = 0, schedule = AUTO or threads_per_track = 0 and the same
+ * update, flags, bsize, layout and masking use them.  A different bsize or layout is a different data layout, which only
  * the caller can adopt (p2z_relayout_device).  Synchronous. */
 p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
                         const uint32_t *d_hit_mask, int reps, p2z_tune_entry *entries, int max_entries,

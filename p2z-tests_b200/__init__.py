@@ -23,7 +23,7 @@ PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = pathlib.Path(os.environ.get("P2Z_LIBRARY", PKG_DIR / "libp2z.so"))
 INCLUDE_H = PKG_DIR.parent / "include" / "p2z.h"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 KFACT_DEFAULT = np.float32(100.0 / (-0.299792458 * 3.8112))
 TRK_WORDS = 28
 HIT_WORDS = 9
@@ -67,7 +67,7 @@ class Config(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("bsize", C.c_int32), ("nevts", C.c_int64), ("ntrks", C.c_int64),
                 ("nlayer", C.c_int32), ("niter", C.c_int32), ("kfact", C.c_float), ("update", C.c_int32),
                 ("schedule", C.c_int32), ("block_threads", C.c_int32), ("flags", C.c_uint32),
-                ("layout", C.c_int32), ("event_ntrks", C.POINTER(C.c_int64))]
+                ("layout", C.c_int32), ("event_ntrks", C.POINTER(C.c_int64)), ("threads_per_track", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -123,7 +123,7 @@ class ValidationPartial(C.Structure):
 
 class TuneEntry(C.Structure):
     _fields_ = [("bsize", C.c_int32), ("layout", C.c_int32), ("schedule", C.c_int32), ("block_threads", C.c_int32),
-                ("ms", C.c_double), ("updates_per_s", C.c_double)]
+                ("threads_per_track", C.c_int32), ("ms", C.c_double), ("updates_per_s", C.c_double)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}
@@ -327,7 +327,8 @@ def hits_to_aos(hits: np.ndarray) -> dict:
 
 
 def make_config(bsize=32, nevts=1, ntrks=None, nlayer=20, niter=1, kfact=0.0, update=UPDATE_V2,
-                schedule=SCHED_AUTO, block_threads=0, flags=0, event_ntrks=None, layout=LAYOUT_AOSOA):
+                schedule=SCHED_AUTO, block_threads=0, flags=0, event_ntrks=None, layout=LAYOUT_AOSOA,
+                threads_per_track=0):
     cfg = Config()
     cfg.abi_version = ABI_VERSION
     cfg.bsize = bsize
@@ -341,6 +342,7 @@ def make_config(bsize=32, nevts=1, ntrks=None, nlayer=20, niter=1, kfact=0.0, up
     cfg.block_threads = block_threads
     cfg.flags = flags
     cfg.layout = LAYOUT_NAMES.get(layout, layout) if isinstance(layout, str) else layout
+    cfg.threads_per_track = threads_per_track
     if event_ntrks is not None:
         arr = np.ascontiguousarray(event_ntrks, dtype=np.int64)
         cfg._event_ntrks_keep = arr  # keep alive with the struct

@@ -50,7 +50,7 @@ struct DevBuf {
 
 struct GraphKey {
   RunArgs args;
-  int bsize, upd, sc, block, grid, kind;
+  int bsize, upd, sc, block, grid, kind, tpt;
   bool masked, soa;
   bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
 };
@@ -59,7 +59,7 @@ struct GraphKey {
 struct Tuned {
   int upd, sc, B;
   bool soa, masked;
-  int block, schedule;
+  int block, schedule, tpt;
 };
 
 }  // namespace
@@ -137,6 +137,7 @@ struct Plan {
   int sc = SC_FAST;
   int schedule = P2Z_SCHED_FLAT;
   int block = 0;
+  int tpt = 1;               // threads per track
   uint32_t flags = 0;
   int64_t nbatches = 0;
   int64_t nslots = 0;
@@ -175,6 +176,14 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
   }
   pl.sc = (cfg->flags & P2Z_FLAG_ACCURATE_TRIG) ? SC_ACCURATE : SC_FAST;
   pl.block = cfg->block_threads ? cfg->block_threads : 128;
+  if (cfg->threads_per_track < 0 || cfg->threads_per_track > 2)
+    return fail(ctx, P2Z_UNSUPPORTED, "threads_per_track %d not in {0, 1, 2}", cfg->threads_per_track);
+  if (cfg->threads_per_track == 2 && pl.upd != UPDK_V2)
+    return fail(ctx, P2Z_UNSUPPORTED, "threads_per_track 2 applies to P2Z_UPDATE_V2 without "
+                                      "P2Z_FLAG_REFERENCE_ROUNDING only");
+  if (cfg->threads_per_track == 2 && cfg->schedule == P2Z_SCHED_STAGED)
+    return fail(ctx, P2Z_UNSUPPORTED, "the staged schedule has one thread per track");
+  pl.tpt = cfg->threads_per_track == 2 ? 2 : 1;
   pl.ev_slot_begin.assign((size_t)cfg->nevts + 1, 0);
   if (cfg->event_ntrks) {
     pl.uneven = true;
@@ -293,6 +302,9 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   spec.masked = base.mask != nullptr;
   spec.block = pl.block;
   spec.grid = 0;
+  spec.tpt = pl.tpt;
+  if (pl.tpt != 1 && schedule == P2Z_SCHED_STAGED)
+    return fail(ctx, P2Z_UNSUPPORTED, "the staged schedule has one thread per track");
   if (schedule == P2Z_SCHED_PER_EVENT) {
     spec.kind = KIND_FLAT;
     const bool spread = (pl.flags & P2Z_FLAG_PER_EVENT_STREAMS) != 0;
@@ -358,7 +370,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
                                       "track and hit arrays");
   const int occ = occupancy(spec);
   if (occ <= 0) return fail(ctx, P2Z_CUDA_ERROR, "occupancy query failed for the persistent kernel");
-  const int64_t items = (s1 - s0 + 31) / 32;
+  const int64_t items = (s1 - s0 + 32 / spec.tpt - 1) / (32 / spec.tpt);
   const int64_t warps_per_cta = spec.block / 32;
   spec.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * ctx->num_sms, (items + warps_per_cta - 1) / warps_per_cta));
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -382,6 +394,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   key.masked = spec.masked;
   key.soa = spec.soa;
   key.kind = spec.kind;
+  key.tpt = spec.tpt;
   if (!(ctx->has_graph && ctx->gkey == key)) {
     if (ctx->gexec) {
       cudaGraphExecDestroy(ctx->gexec);
@@ -417,7 +430,9 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
 }
 
 // Applies the autotuner's measurement for this kind of run to the fields the
-// caller left open (block_threads = 0, schedule = AUTO), then resolves AUTO.
+// caller left open (block_threads = 0, schedule = AUTO, threads_per_track =
+// 0), then resolves AUTO.  A tuned shape whose schedule the caller overrides
+// with STAGED keeps one thread per track.
 int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool masked) {
   masked = masked || pl.uneven;
   if (ctx) {
@@ -425,6 +440,7 @@ int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool mas
       if (t.upd == pl.upd && t.sc == pl.sc && t.B == pl.B && t.soa == pl.soa && t.masked == masked) {
         if (cfg->block_threads == 0) pl.block = t.block;
         if (pl.schedule == P2Z_SCHED_AUTO) pl.schedule = t.schedule;
+        if (cfg->threads_per_track == 0 && pl.schedule != P2Z_SCHED_STAGED) pl.tpt = t.tpt;
         break;
       }
     }
@@ -515,11 +531,11 @@ p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg) { retu
 void *context_scratch(p2z_context *ctx, size_t bytes) {
   return ensure(ctx, ctx->aux, bytes) == P2Z_OK ? ctx->aux.p : nullptr;
 }
-p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule) {
+p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt) {
   Plan pl;
   p2z_status r = make_plan(ctx, cfg, pl);
   if (r != P2Z_OK) return r;
-  Tuned t{pl.upd, pl.sc, pl.B, pl.soa, masked || pl.uneven, block, schedule};
+  Tuned t{pl.upd, pl.sc, pl.B, pl.soa, masked || pl.uneven, block, schedule, tpt};
   for (Tuned &o : ctx->tuned) {
     if (o.upd == t.upd && o.sc == t.sc && o.B == t.B && o.soa == t.soa && o.masked == t.masked) {
       o = t;

@@ -129,12 +129,23 @@ __device__ __forceinline__ void load_hit(HitRegs<NH> &h, const float *p, int64_t
   for (int e = 0; e < NH; ++e) h.w[e] = __ldg(p + e * ws);
 }
 
+// A thread's place in its track: with TPT = 2 threads per track, lanes 2i and
+// 2i+1 hold the same track; j is this lane's component of the split
+// covariance propagation (propagate_cov_reduced_pair) and pm the pair's lanes.
+struct PairLane {
+  bool j = false;
+  unsigned pm = 0xffffffffu;
+};
+
 // One propagate + update step.  GENERAL: first present layer (full 21-element
-// input covariance in b21).  Returns true if the update met det <= 0.
-template <int UPD, int SC, bool GENERAL>
+// input covariance in b21).  TPT = 2 (UPDK_V2 only): the propagation of the
+// covariance is split over the lane pair; everything else is evaluated by both
+// lanes.  Returns true if the update met det <= 0.
+template <int UPD, int SC, bool GENERAL, int TPT = 1>
 __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<UPD>::A> &s,
                                      const typename Types<UPD>::T *b21, const HitRegs<Types<UPD>::NH> &h,
-                                     typename Types<UPD>::T k, typename Types<UPD>::T ik) {
+                                     typename Types<UPD>::T k, typename Types<UPD>::T ik, PairLane ln = {}) {
+  static_assert(TPT == 1 || (TPT == 2 && UPD == UPDK_V2), "two threads per track: UPDK_V2 only");
   using T = typename Types<UPD>::T;
   const T zout = T(h.w[2]);
   Helix<T> hx;
@@ -150,6 +161,7 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
     J = jacobian_precise<float, GENERAL>(hx, k, s.ipt);
   }
   if constexpr (GENERAL) propagate_cov_general(s, b21, hx, J);
+  else if constexpr (TPT == 2) propagate_cov_reduced_pair(s, J, ln.j, ln.pm);
   else if constexpr (P2Z_PACKED_F32X2 && std::is_same<T, float>::value && UPD != UPDK_V2_REF)
     propagate_cov_reduced_packed(s, J);  // (the reference-rounding form keeps separate roundings)
   else propagate_cov_reduced(s, J);
@@ -173,8 +185,9 @@ __device__ __forceinline__ bool step(Trk<typename Types<UPD>::T, typename Types<
   }
 }
 
-// Process one track slot: load, run every present layer, store.
-template <int B, int UPD, int SC, bool MASKED>
+// Process one track slot: load, run every present layer, store.  TPT = 2: both
+// lanes of the pair load the track and its hits, and lane 0 stores the result.
+template <int B, int UPD, int SC, bool MASKED, int TPT = 1>
 __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   using T = typename Types<UPD>::T;
   using A = typename Types<UPD>::A;
@@ -183,6 +196,12 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   const float *tin = trk_lane<B>(a.trk, slot);
   float *tout = const_cast<float *>(trk_lane<B>(a.out, slot));
 
+  PairLane ln;
+  if constexpr (TPT == 2) {
+    ln.j = (threadIdx.x & 1) != 0;
+    ln.pm = 3u << (threadIdx.x & 30);
+  }
+  const bool writer = TPT == 1 || !ln.j;
   const uint32_t all = (a.nlayer >= 32) ? 0xffffffffu : ((1u << a.nlayer) - 1u);
   uint32_t m = MASKED ? (__ldg(a.mask + slot) & all) : all;
 
@@ -191,8 +210,10 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   for (int e = 0; e < TRK_WORDS; ++e) in[e] = __ldg(tin + e * WS);
 
   if (m == 0u) {  // no hits (or a padding slot): the track passes through
+    if (writer) {
 #pragma unroll
-    for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, in[e]);
+      for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, in[e]);
+    }
     return;
   }
 
@@ -223,28 +244,28 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
     load_hit<NH>(h0, hp, WS);
     if (nl > 1) load_hit<NH>(h1, hp + stride, WS);
     if (nl > 2) load_hit<NH>(h2, hp + 2 * stride, WS);
-    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    singular |= step<UPD, SC, true, TPT>(s, b21, h0, k, ik, ln);
     int l = 1;
     for (; l + 2 < nl; l += 3) {  // layers l, l+1, l+2 are in h1, h2 and (after the load) h0
       if (l + 2 < nl) load_hit<NH>(h0, hp + (l + 2) * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
       if (l + 3 < nl) load_hit<NH>(h1, hp + (l + 3) * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h2, k, ik, ln);
       if (l + 4 < nl) load_hit<NH>(h2, hp + (l + 4) * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h0, k, ik, ln);
     }
-    if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
-    if (l + 1 < nl) singular |= step<UPD, SC, false>(s, b21, h2, k, ik);
+    if (l < nl) singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
+    if (l + 1 < nl) singular |= step<UPD, SC, false, TPT>(s, b21, h2, k, ik, ln);
   } else if constexpr (!MASKED && P2Z_PREFETCH_DEPTH == 0) {
     // every layer present, one hit buffer: each layer's hits are loaded at the
     // start of its step (latency hidden by other warps only)
     const int64_t stride = HIT_WORDS * WS;
     const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0, WS);
     load_hit<NH>(h0, hp, WS);
-    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    singular |= step<UPD, SC, true, TPT>(s, b21, h0, k, ik, ln);
     for (int l = 1; l < a.nlayer; ++l) {
       load_hit<NH>(h0, hp + l * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h0, k, ik, ln);
     }
   } else if constexpr (!MASKED) {
     // every layer present: counted loop, hits addressed by a running pointer;
@@ -254,29 +275,29 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
     const int nl = a.nlayer;
     load_hit<NH>(h0, hp, WS);
     if (nl > 1) load_hit<NH>(h1, hp + stride, WS);
-    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    singular |= step<UPD, SC, true, TPT>(s, b21, h0, k, ik, ln);
     int l = 1;
     for (; l + 1 < nl; l += 2) {
       load_hit<NH>(h0, hp + (l + 1) * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
       if (l + 2 < nl) load_hit<NH>(h1, hp + (l + 2) * stride, WS);
-      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h0, k, ik, ln);
     }
-    if (l < nl) singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+    if (l < nl) singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
   } else {
     // present layers in order: lowest set bit first
     uint32_t rest = m & (m - 1u);
     load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(m) - 1, WS), WS);
     if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
-    singular |= step<UPD, SC, true>(s, b21, h0, k, ik);
+    singular |= step<UPD, SC, true, TPT>(s, b21, h0, k, ik, ln);
     while (rest) {
       rest &= rest - 1u;  // h1 holds the layer just removed from rest
       if (rest) load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
-      singular |= step<UPD, SC, false>(s, b21, h1, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
       if (!rest) break;
       rest &= rest - 1u;  // h0 holds the layer just removed
       if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
-      singular |= step<UPD, SC, false>(s, b21, h0, k, ik);
+      singular |= step<UPD, SC, false, TPT>(s, b21, h0, k, ik, ln);
     }
   }
 
@@ -292,37 +313,40 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   c[15] = float(s.c50); c[16] = float(s.c51); c[17] = z0; c[18] = float(s.c53); c[19] = float(s.c54);
   c[20] = float(s.c55);
   o[27] = in[27];
+  if (writer) {
 #pragma unroll
-  for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, o[e]);
-  if (singular) atomicOr(a.status, 1u);
+    for (int e = 0; e < TRK_WORDS; ++e) __stcs(tout + e * WS, o[e]);
+    if (singular) atomicOr(a.status, 1u);
+  }
 }
 
 
 
-// One launch over slots [slot_begin, slot_end), one thread per slot.
-template <int B, int UPD, int SC, bool MASKED>
+// One launch over slots [slot_begin, slot_end), TPT threads per slot.
+template <int B, int UPD, int SC, bool MASKED, int TPT = 1>
 __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_flat(RunArgs a) {
-  const int64_t slot = a.slot_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= a.slot_end) return;
-  process_slot<B, UPD, SC, MASKED>(a, MASKED ? map_slot(a, slot) : slot);
+  const int64_t slot = a.slot_begin + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / TPT;
+  if (slot >= a.slot_end) return;  // (both lanes of a pair together)
+  process_slot<B, UPD, SC, MASKED, TPT>(a, MASKED ? map_slot(a, slot) : slot);
 }
 
 // Persistent launch: grid = resident CTAs; each warp repeatedly takes the next
-// 32-slot work item from a device counter (reset to 0 before the launch) until
-// the range is exhausted.  Work items are taken in slot order, so concurrently
-// running warps read neighbouring batches.
-template <int B, int UPD, int SC, bool MASKED>
+// work item of 32 / TPT slots from a device counter (reset to 0 before the
+// launch) until the range is exhausted.  Work items are taken in slot order,
+// so concurrently running warps read neighbouring batches.
+template <int B, int UPD, int SC, bool MASKED, int TPT = 1>
 __global__ void __launch_bounds__(256, Types<UPD>::MIN_CTAS) k_persistent(RunArgs a) {
+  constexpr int kPer = 32 / TPT;  // slots per work item
   const int lane = threadIdx.x & 31;
   const int64_t nslots = a.slot_end - a.slot_begin;
-  const unsigned long long nitems = (unsigned long long)((nslots + 31) / 32);
+  const unsigned long long nitems = (unsigned long long)((nslots + kPer - 1) / kPer);
   for (;;) {
     unsigned long long item = 0;
     if (lane == 0) item = atomicAdd(a.queue, 1ull);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nitems) break;
-    const int64_t slot = a.slot_begin + (int64_t)item * 32 + lane;
-    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED>(a, MASKED ? map_slot(a, slot) : slot);
+    const int64_t slot = a.slot_begin + (int64_t)item * kPer + lane / TPT;
+    if (slot < a.slot_end) process_slot<B, UPD, SC, MASKED, TPT>(a, MASKED ? map_slot(a, slot) : slot);
   }
 }
 
@@ -622,6 +646,7 @@ struct LaunchSpec {
   int kind;      // KIND_*
   int block;     // threads per CTA
   int grid;      // CTAs (persistent); flat computes its own
+  int tpt;       // threads per track: 1, or 2 (UPDK_V2, flat and persistent kinds)
 };
 
 // Per-update-kind dispatchers (one translation unit each).
@@ -639,15 +664,24 @@ int occupancy_3x3_comp(const LaunchSpec &s);
 int occupancy_f64(const LaunchSpec &s);
 int occupancy_v2_ref(const LaunchSpec &s);
 
-// Shared dispatch body: picks the template instance for (B, SC, MASKED, KIND).
+// Shared dispatch body: picks the template instance for (B, SC, MASKED, KIND,
+// threads per track).
 template <int UPD, bool HAS_FAST>
 struct Dispatch {
+  static constexpr bool HAS_PAIR = UPD == UPDK_V2;
   template <int B, int SC, bool M>
-  static const void *fn(int kind) {
+  static const void *fn(int kind, int tpt) {
     if (kind == KIND_STAGED) {
-      if constexpr (B == 32) return (const void *)k_staged<UPD, SC, M>;
+      if constexpr (B == 32) return tpt == 1 ? (const void *)k_staged<UPD, SC, M> : nullptr;
       else return nullptr;
     }
+    if (tpt == 2) {
+      if constexpr (HAS_PAIR)
+        return kind == KIND_PERSISTENT ? (const void *)k_persistent<B, UPD, SC, M, 2>
+                                       : (const void *)k_flat<B, UPD, SC, M, 2>;
+      else return nullptr;
+    }
+    if (tpt != 1) return nullptr;
     return kind == KIND_PERSISTENT ? (const void *)k_persistent<B, UPD, SC, M> : (const void *)k_flat<B, UPD, SC, M>;
   }
   // dynamic shared memory of a launch
@@ -655,23 +689,23 @@ struct Dispatch {
     return s.kind == KIND_STAGED ? (size_t)(s.block / 32) * StagedSmem<UPD>::kWarpBytes : 0;
   }
   template <int B, int SC>
-  static const void *fn_m(bool masked, int kind) {
-    return masked ? fn<B, SC, true>(kind) : fn<B, SC, false>(kind);
+  static const void *fn_m(bool masked, int kind, int tpt) {
+    return masked ? fn<B, SC, true>(kind, tpt) : fn<B, SC, false>(kind, tpt);
   }
   template <int B>
-  static const void *fn_sc(int sc, bool masked, int kind) {
+  static const void *fn_sc(int sc, bool masked, int kind, int tpt) {
     if constexpr (HAS_FAST) {
-      if (sc == SC_FAST) return fn_m<B, SC_FAST>(masked, kind);
+      if (sc == SC_FAST) return fn_m<B, SC_FAST>(masked, kind, tpt);
     }
-    return fn_m<B, SC_ACCURATE>(masked, kind);
+    return fn_m<B, SC_ACCURATE>(masked, kind, tpt);
   }
   static const void *select(const LaunchSpec &s) {
-    if (s.soa) return fn_sc<0>(s.sc, s.masked, s.kind);
+    if (s.soa) return fn_sc<0>(s.sc, s.masked, s.kind, s.tpt);
     switch (s.bsize) {
-      case 8: return fn_sc<8>(s.sc, s.masked, s.kind);
-      case 16: return fn_sc<16>(s.sc, s.masked, s.kind);
-      case 32: return fn_sc<32>(s.sc, s.masked, s.kind);
-      case 64: return fn_sc<64>(s.sc, s.masked, s.kind);
+      case 8: return fn_sc<8>(s.sc, s.masked, s.kind, s.tpt);
+      case 16: return fn_sc<16>(s.sc, s.masked, s.kind, s.tpt);
+      case 32: return fn_sc<32>(s.sc, s.masked, s.kind, s.tpt);
+      case 64: return fn_sc<64>(s.sc, s.masked, s.kind, s.tpt);
       default: return nullptr;
     }
   }
@@ -684,7 +718,7 @@ struct Dispatch {
     if (s.kind == KIND_PERSISTENT || s.kind == KIND_STAGED) {
       grid = s.grid;
     } else {
-      grid = (int)((n + s.block - 1) / s.block);
+      grid = (int)((n * s.tpt + s.block - 1) / s.block);
     }
     const size_t smem = smem_bytes(s);
     if (smem > 48 * 1024) {

@@ -568,6 +568,48 @@ __device__ __forceinline__ void propagate_cov_reduced_packed(Trk<float, A> &s, c
   s.c54 = t29;
 }
 
+// Two threads per track: lanes 2i (j = 0) and 2i+1 (j = 1) of a warp hold the
+// same track.  Each lane evaluates component j of every pair of the packed
+// form above -- row j of T = J C and of the propagated measured columns -- as
+// one scalar fused multiply-add per packed one, in the same order, and takes
+// the other component from its partner lane with one shuffle per pair, so
+// both lanes end with the packed form's results bit for bit.  The scalar
+// chains (t7, t27..t29, c44) are evaluated by both lanes; c11 needs row 1 of
+// T, which lane 1 holds, and comes from there.  pm names the two lanes.
+__device__ __forceinline__ void pair_join(float own, bool j, unsigned pm, float &x, float &y) {
+  const float other = __shfl_xor_sync(pm, own, 1);
+  x = j ? other : own;
+  y = j ? own : other;
+}
+
+template <typename A>
+__device__ __forceinline__ void propagate_cov_reduced_pair(Trk<float, A> &s, const Jac<float> &J, bool j,
+                                                           unsigned pm) {
+  const float A3 = j ? J.a9 : J.a3, A4 = j ? J.a10 : J.a4, A5 = j ? J.a11 : J.a5;
+  const float P0 = j ? s.c10 : s.c00, P3 = j ? s.c31 : s.c30, P4 = j ? s.c41 : s.c40, P5 = j ? s.c51 : s.c50;
+  const float T0 = fmaf(A5, s.c50, fmaf(A4, s.c40, fmaf(A3, s.c30, P0)));  // t0 | t6
+  const float T3 = fmaf(A5, s.c53, fmaf(A4, s.c43, fmaf(A3, s.c33, P3)));  // t3 | t9
+  const float T4 = fmaf(A5, s.c54, fmaf(A4, s.c44, fmaf(A3, s.c43, P4)));  // t4 | t10
+  const float T5 = fmaf(A5, s.c55, fmaf(A4, s.c54, fmaf(A3, s.c53, P5)));  // t5 | t11
+  const float t7 = s.c11 + J.a9 * s.c31 + J.a10 * s.c41 + J.a11 * s.c51;
+  const float T24 = fmaf(J.a29, P5, fmaf(J.a27, P3, P4));                  // t24 | t25
+  const float t27 = J.a27 * s.c33 + s.c43 + J.a29 * s.c53;
+  const float t28 = J.a27 * s.c43 + s.c44 + J.a29 * s.c54;
+  const float t29 = J.a27 * s.c53 + s.c54 + J.a29 * s.c55;
+  const float N0 = fmaf(T5, J.a5, fmaf(T4, J.a4, fmaf(T3, J.a3, T0)));    // c00 | c10
+  const float c11 = t7 + T3 * J.a9 + T4 * J.a10 + T5 * J.a11;              // the result on lane 1
+  const float N4 = fmaf(A5, t29, fmaf(A4, t28, fmaf(A3, t27, T24)));       // c40 | c41
+  pair_join(N0, j, pm, s.c00, s.c10);
+  pair_join(T3, j, pm, s.c30, s.c31);
+  pair_join(N4, j, pm, s.c40, s.c41);
+  pair_join(T5, j, pm, s.c50, s.c51);
+  const float c11o = __shfl_xor_sync(pm, c11, 1);
+  s.c11 = j ? c11 : c11o;
+  s.c43 = t27;
+  s.c44 = t27 * J.a27 + t28 + t29 * J.a29;
+  s.c54 = t29;
+}
+
 // General form on the full 21-element input covariance b[] (the first
 // propagation of a track), including the Jacobian's z column a2 = J(0,2),
 // a8 = J(1,2), a26 = J(4,2) (reference :655, :659, :663), which the Jacobian

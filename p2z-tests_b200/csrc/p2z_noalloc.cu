@@ -203,6 +203,7 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
   }
   LaunchSpec spec;
   std::memset(&spec, 0, sizeof spec);
+  spec.tpt = 1;
   spec.args.trk = static_cast<const float *>(d_trk_in);
   spec.args.hits = static_cast<const float *>(d_hits);
   spec.args.out = static_cast<float *>(d_trk_out);

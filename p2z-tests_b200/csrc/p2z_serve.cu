@@ -198,6 +198,7 @@ void launch_group(p2z_server *s) {
   // contiguous runs of ring batches (a run breaks where the ring wraps)
   LaunchSpec spec;
   std::memset(&spec, 0, sizeof spec);
+  spec.tpt = 1;
   spec.args.trk = s->d_trk;
   spec.args.hits = s->d_hit;
   spec.args.out = s->d_out;

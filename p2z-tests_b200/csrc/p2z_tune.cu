@@ -1,6 +1,6 @@
 // p2z_tune.cu -- layout conversion between bsizes / AOSOA / SoA on the device,
-// and the autotuner that measures every (bsize, layout, schedule, block size)
-// on the caller's data.  Neither has a counterpart in the reference, whose
+// and the autotuner that measures every (bsize, layout, schedule, block size,
+// threads per track) on the caller's data.  Neither has a counterpart in the reference, whose
 // bsize is a compile-time macro (src/propagate-toz-test_OMP.cpp:22-24) and
 // whose launch shape is fixed per build (src/propagate-toz-test_CUDA_v4.cu:
 // 57-72).
@@ -19,7 +19,7 @@ void set_context_free_error(const char *msg);
 int context_device(const p2z_context *ctx);
 cudaStream_t context_stream(const p2z_context *ctx);
 p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg);
-p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule);
+p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt);
 }  // namespace p2z
 
 using namespace p2z;
@@ -196,6 +196,8 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
   static const int kBlock[] = {32, 64, 128, 256};
   std::vector<int> scheds = {P2Z_SCHED_FLAT, P2Z_SCHED_PERSISTENT};
   if (cfg->nevts <= 4096) scheds.push_back(P2Z_SCHED_PER_EVENT);
+  // two threads per track: the precise 2-D update, every schedule but STAGED
+  const bool pair_ok = cfg->update == P2Z_UPDATE_V2 && !(cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING);
 
   // candidate configs per bsize: uniform when ntrks divides, else uneven with
   // the same per-event counts
@@ -248,42 +250,53 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
       p2z_config cu = c;
       cu.schedule = P2Z_SCHED_FLAT;
       cu.block_threads = 128;
+      cu.threads_per_track = 1;
       p2z_stats s0;
       r = p2z_run_device(ctx, &cu, T, H, (const uint32_t *)M, O, st, &s0);
       if (r != P2Z_OK) return r;
       p2z_tune_entry local;
       std::memset(&local, 0, sizeof local);
       local.ms = -1.0;
-      for (int sched : sch) {
-        for (int block : kBlock) {
-          c.schedule = sched;
-          c.block_threads = block;
-          r = p2z_run_device(ctx, &c, T, H, (const uint32_t *)M, O, st, nullptr);  // warm-up (graph capture)
+      // every (schedule, threads per track, block size) of this bsize and layout
+      struct Shape {
+        int sched, tpt, block;
+      };
+      std::vector<Shape> shapes;
+      for (int sched : sch)
+        for (int tpt = 1; tpt <= ((pair_ok && sched != P2Z_SCHED_STAGED) ? 2 : 1); ++tpt)
+          for (int block : kBlock) shapes.push_back({sched, tpt, block});
+      for (const Shape &sh : shapes) {
+        c.schedule = sh.sched;
+        c.block_threads = sh.block;
+        c.threads_per_track = sh.tpt;
+        r = p2z_run_device(ctx, &c, T, H, (const uint32_t *)M, O, st, nullptr);  // warm-up (graph capture)
+        if (r != P2Z_OK) return r;
+        TUNE_CUDA(ctx, cudaEventRecord(e0, st));
+        for (int i = 0; i < reps; ++i) {
+          r = p2z_run_device(ctx, &c, T, H, (const uint32_t *)M, O, st, nullptr);
           if (r != P2Z_OK) return r;
-          TUNE_CUDA(ctx, cudaEventRecord(e0, st));
-          for (int i = 0; i < reps; ++i) {
-            r = p2z_run_device(ctx, &c, T, H, (const uint32_t *)M, O, st, nullptr);
-            if (r != P2Z_OK) return r;
-          }
-          TUNE_CUDA(ctx, cudaEventRecord(e1, st));
-          TUNE_CUDA(ctx, cudaEventSynchronize(e1));
-          float ms = 0.f;
-          TUNE_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
-          p2z_tune_entry t;
-          t.bsize = B;
-          t.layout = layout;
-          t.schedule = sched;
-          t.block_threads = block;
-          t.ms = ms / reps;
-          t.updates_per_s = t.ms > 0 ? (double)s0.updates / (t.ms * 1e-3) : 0.0;
-          if (n < max_entries) entries[n] = t;
-          ++n;
-          if (local.ms < 0 || t.ms < local.ms) local = t;
         }
+        TUNE_CUDA(ctx, cudaEventRecord(e1, st));
+        TUNE_CUDA(ctx, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        TUNE_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+        p2z_tune_entry t;
+        std::memset(&t, 0, sizeof t);
+        t.bsize = B;
+        t.layout = layout;
+        t.schedule = sh.sched;
+        t.block_threads = sh.block;
+        t.threads_per_track = sh.tpt;
+        t.ms = ms / reps;
+        t.updates_per_s = t.ms > 0 ? (double)s0.updates / (t.ms * 1e-3) : 0.0;
+        if (n < max_entries) entries[n] = t;
+        ++n;
+        if (local.ms < 0 || t.ms < local.ms) local = t;
       }
       c.schedule = P2Z_SCHED_AUTO;
       c.block_threads = 0;
-      r = record_tuned(ctx, &c, masked, local.block_threads, local.schedule);
+      c.threads_per_track = 0;
+      r = record_tuned(ctx, &c, masked, local.block_threads, local.schedule, local.threads_per_track);
       if (r != P2Z_OK) return r;
       if (top.ms < 0 || local.ms < top.ms) top = local;
     }

@@ -205,7 +205,11 @@ def test_autotune_contract(p2z, masked):
         c.run_device(cfg, dt, dh, ref, d_mask=dm, stats=False)
         torch.cuda.synchronize()
         best, rows = c.autotune(cfg, dt, dh, d_mask=dm, reps=2)
-        assert len(rows) == 4 * 2 * 3 * 4 + 4  # + the staged schedule at bsize 32 AOSOA
+        # bsize x layout x (flat, persistent, per-event) x threads per track {1, 2} x block,
+        # + the staged schedule (one thread per track) at bsize 32 AOSOA
+        assert len(rows) == 4 * 2 * 3 * 2 * 4 + 4
+        assert {r["threads_per_track"] for r in rows} == {1, 2}
+        assert {r["threads_per_track"] for r in rows if r["schedule"] == "staged"} == {1}
         assert {r["bsize"] for r in rows} == {8, 16, 32, 64}
         assert {r["layout"] for r in rows} == {"aosoa", "soa"}
         assert {r["schedule"] for r in rows} == {"flat", "persistent", "per_event", "staged"}
@@ -213,7 +217,7 @@ def test_autotune_contract(p2z, masked):
         assert {r["block_threads"] for r in rows} == {32, 64, 128, 256}
         assert best["ms"] == min(r["ms"] for r in rows) and best["ms"] > 0
         assert all(r["updates_per_s"] > 0 for r in rows)
-        # later runs with open block/schedule at bsize 32, AOSOA use the tuned shape
+        # later runs with open block/schedule/threads per track at bsize 32, AOSOA use the tuned shape
         mine = min((r for r in rows if r["bsize"] == 32 and r["layout"] == "aosoa"), key=lambda r: r["ms"])
         out = torch.empty_like(dt)
         st = c.run_device(cfg, dt, dh, out, d_mask=dm)
