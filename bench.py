@@ -293,6 +293,33 @@ def tune_summary(best, rows, wall_s):
     return out
 
 
+def small_run_latency(p2z, ctx, t, h, o):
+    """Host wall time of one synchronous p2z_run call on a lone event of 1024
+    or 9600 tracks from page-locked buffers (the first batches of the bench
+    sample): the pipeline replayed as a recorded graph against the same
+    pipeline enqueued copy by copy (P2Z_FLAG_NO_GRAPH); mean of 200 calls
+    after 5 warm-up calls."""
+    out = {}
+    for n in (1024, 9600):
+        nb = n // 32
+        row = {}
+        for mode, flags in (("graph", 0), ("direct", p2z.FLAG_NO_GRAPH)):
+            cfg = p2z.make_config(bsize=32, nevts=1, ntrks=n, nlayer=20, schedule="flat", flags=flags)
+            args = (ctx.h, p2z.C.byref(cfg), t[:nb].ctypes.data, h[:nb].ctypes.data, None, o[:nb].ctypes.data, None)
+            for _ in range(5):
+                p2z.lib.p2z_run(*args)
+            t0 = time.perf_counter()
+            for _ in range(200):
+                rc = p2z.lib.p2z_run(*args)
+            us = (time.perf_counter() - t0) / 200 * 1e6
+            if rc != p2z.OK:
+                raise p2z.P2zError(rc, p2z.lib.p2z_last_error(ctx.h).decode())
+            row[mode + "_us"] = us
+        out[str(n)] = row
+    return {"note": "p2z_run from page-locked buffers, one event, host wall time per synchronous call",
+            "tracks": out}
+
+
 def threads_per_track_report(p2z, ctx, torch, dt, dh, do, stream):
     """One thread per track against two (p2z_config.threads_per_track), flat
     launches of the precise form at bsize 32 AOSOA: (1) throughput on the
@@ -708,6 +735,8 @@ def main():
                             "peak_source": "measured in this run: p2z_measure_peaks, one 1 GiB pinned "
                                            "cudaMemcpyAsync each way and both at once, best of 5"}}
         out_ok = bool(np.isfinite(pin_o.array[:, :6, :]).all())
+        if rank == 0:
+            e2e["small_runs"] = small_run_latency(p2z, ctx, pin_t.array, pin_h.array, pin_o.array)
         pin_t.free(); pin_h.free(); pin_o.free()
     else:
         del dt, dh, do

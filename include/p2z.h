@@ -121,7 +121,8 @@ typedef enum p2z_layout {
 /* Flags */
 #define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan inputs for NaN/Inf first -> P2Z_NONFINITE_INPUT */
 #define P2Z_FLAG_STRICT       0x2u  /* return P2Z_SINGULAR if any det <= 0 was met */
-#define P2Z_FLAG_NO_GRAPH     0x4u  /* PERSISTENT: launch directly instead of replaying a graph */
+#define P2Z_FLAG_NO_GRAPH     0x4u  /* PERSISTENT, and p2z_run with page-locked buffers: enqueue
+                                       directly instead of replaying a recorded graph */
 #define P2Z_FLAG_ACCURATE_TRIG 0x8u /* sin and 1 - cos of every per-layer angle from sincosf of its
                                        half (default: Taylor polynomials for the helix angle alpha
                                        when |alpha| <= 0.5, for cosP*sin(alpha) and for the phi
@@ -233,7 +234,15 @@ size_t p2z_sizeof_mphit(int bsize);   /* 9*bsize*4 */
  *   hit_mask uint32[nbatches*bsize]     (host, optional, see above)
  *   trk_out  MPTRK[nbatches]            (host; may equal trk_in)
  * Host buffers that are page-locked (cudaHostAlloc / p2z_host_alloc) are
- * copied asynchronously; pageable ones go through a staging path. */
+ * copied asynchronously; pageable ones go through a staging path.  The work is
+ * split into up to 8 chunks whose copies and passes alternate between two
+ * streams.  With page-locked buffers (all of trk_in, hits, trk_out and
+ * hit_mask when given) the whole pipeline is recorded as a CUDA graph on the
+ * first call and replayed by later calls with the same config, host buffers
+ * and internal device buffers, so that a call costs one graph launch; a call
+ * that differs in any of them records again.  P2Z_FLAG_NO_GRAPH enqueues
+ * every copy and kernel directly.  Synchronous: returns when trk_out holds
+ * the results. */
 p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, const void *hits,
                    const uint32_t *hit_mask, void *trk_out, p2z_stats *stats);
 
