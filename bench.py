@@ -251,7 +251,7 @@ def order_by_hits(torch, counts, udt, udh, udm):
 
 
 def window_util(mask, win):
-    """Lane utilisation of a masked run whose 256-slot windows are processed
+    """Lane utilisation of a masked run whose `win`-slot windows are processed
     in order of hit count: present-hit lane-steps over 32 x the warps' steps."""
     import torch
     m = mask.to(torch.int64) & 0xFFFFFFFF
@@ -790,7 +790,7 @@ def main():
 
         for sched in ("persistent", "per_event"):
             res[sched] = timed(cfg_for(sched), udt, udh, udm, udo)
-        # the same batched run with each 256-slot window in order of hit count (in-library sort)
+        # the same batched run with each 128-slot window in order of hit count (in-library sort)
         csw = cfg_for("persistent")
         csw.flags |= p2z.FLAG_SORT_WINDOWS
         res["persistent_sorted_windows"] = timed(csw, udt, udh, udm, udo)
@@ -817,9 +817,9 @@ def main():
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
                "plain_per_event_launch_10_streams": res["per_event_10_streams"],
                "batched_persistent_graph_sorted_windows": res["persistent_sorted_windows"],
-               "lane_utilisation": {"stored_order": util_packed, "sorted_windows": window_util(udm, 256),
+               "lane_utilisation": {"stored_order": util_packed, "sorted_windows": window_util(udm, 128),
                                     "note": "present-hit lane-steps / (32 x warp steps); sorted_windows: each "
-                                            "256-slot window in order of hit count (P2Z_FLAG_SORT_WINDOWS)"},
+                                            "128-slot window in order of hit count (P2Z_FLAG_SORT_WINDOWS)"},
                "ratio": res["persistent"] / res["per_event"],
                "ratio_vs_10_streams": res["persistent"] / res["per_event_10_streams"],
                "batched_roofline": {

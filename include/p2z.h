@@ -134,15 +134,16 @@ typedef enum p2z_layout {
                                        the reference's GPU build spreads its launches over num_streams
                                        = 10 (src/propagate-toz-test_CUDA_v4.cu:40-41, :972-986); the
                                        default issues them in order on the run's stream */
-#define P2Z_FLAG_SORT_WINDOWS 0x80u /* masked runs, FLAT / PERSISTENT: process each window of 256
+#define P2Z_FLAG_SORT_WINDOWS 0x80u /* masked runs, FLAT / PERSISTENT: process each window of 128
                                        consecutive slots in order of the slots' hit counts (a 1-byte
                                        permutation the run computes on the device), so a warp's 32
                                        tracks take similar numbers of steps.  Per-track results are
-                                       the same.  Off by default: on the uneven benchmark sample the
-                                       lanes' scattered loads cost more than the 60% -> 92% lane
-                                       utilisation saves (measured slower); packing an event's tracks
-                                       in order of hit count when the arrays are built gains without
-                                       that cost */
+                                       the same.  On the uneven benchmark sample lane utilisation
+                                       rises from 60% to 85% and the persistent pass is 13% faster;
+                                       a warp's loads then reach 4 batches, so on even work (every
+                                       mask alike) it only costs.  Packing an event's tracks in order
+                                       of hit count when the arrays are built gains more (99%) and
+                                       costs nothing per pass */
 #define P2Z_FLAG_REFERENCE_ROUNDING 0x20u /* P2Z_UPDATE_V2 only: evaluate the reference's own FP32
                                        expressions, type promotions and operation order, every
                                        operation separately rounded, with correctly rounded

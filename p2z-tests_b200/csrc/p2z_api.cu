@@ -24,11 +24,13 @@ constexpr int kEventStreams = 10;
 // Masked runs with P2Z_FLAG_SORT_WINDOWS: slots per sorted window.
 // A warp's 32 tracks take as many steps as the longest of them; with hit
 // counts of 5-20 per track, 32 slots taken in stored order keep 60% of the
-// lane-steps busy, 256 slots sorted by hit count 92% (32 sorted slots, i.e.
-// no sort, 60%; 64: 74%; 128: 85%).  The window stays within 8 batches of 32,
-// so a warp's loads stay within that many neighbouring batches.
+// lane-steps busy; sorted by hit count, windows of 64, 128 and 256 slots keep
+// 74%, 85% and 92%.  A sorted warp's loads reach as many batches of 32 as the
+// window holds, which costs per step: measured on one B200 (2000-event
+// sample, persistent schedule) 1.725, 1.668 and 2.189 ms against 1.894 ms in
+// stored order, so the window is 128 slots.
 #ifndef P2Z_SORT_WINDOW
-#define P2Z_SORT_WINDOW 256
+#define P2Z_SORT_WINDOW 128
 #endif
 
 namespace p2z {

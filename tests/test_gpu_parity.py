@@ -299,10 +299,10 @@ def test_uneven_events_with_masks(p2z, oracle, ctx):
 
 @pytest.mark.parametrize("schedule", ["flat", "persistent"])
 def test_sorted_windows_bitwise_equal(p2z, ctx, schedule):
-    """Masked runs process each window of 256 slots in order of hit count
+    """Masked runs process each window of 128 slots in order of hit count
     (P2Z_FLAG_SORT_WINDOWS) or in stored order (default): the same bits for every
     track, through the device and the chunked host paths, with a last window
-    that is only partly filled (9 events, 1601 real tracks)."""
+    that is only partly filled (9 events, 1601 real tracks in 1728 slots)."""
     import torch
     counts = np.array([700, 33, 0, 1, 255, 256, 257, 64, 35], dtype=np.int64)
     cfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20, schedule=schedule)
