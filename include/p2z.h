@@ -295,11 +295,10 @@ p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *
  * enqueueing.  The first call on a device looks up the scratch array's device
  * address (once per device, with that device current) and keeps it for the
  * life of the process, so a device that is reset (cudaDeviceReset) must not
- * be used with this entry point afterwards in that process; make that first
- * call before any stream capture.  All calls share the one scratch array and
- * each call resets what must start at zero, so calls whose work overlaps on
- * the GPU (different streams, or concurrent host threads) race on it:
- * serialise them. */
+ * be used with this entry point afterwards in that process.  All calls share
+ * the one scratch array and each call resets what must start at zero, so
+ * calls whose work overlaps on the GPU (different streams, or concurrent host
+ * threads) race on it: serialise them. */
 #define P2Z_NOALLOC_MAX_SLOTS (1 << 20)
 #define P2Z_NOALLOC_MAX_EVENTS (1 << 16)
 p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
