@@ -614,6 +614,10 @@ def main():
     ap.add_argument("--schedule", default="auto", choices=["auto", "flat", "persistent", "per_event", "staged"],
                     help="launch schedule of the headline step (auto: what the autotuner measured best)")
     ap.add_argument("--block", type=int, default=0, help="threads per CTA of the headline step (0: tuned)")
+    ap.add_argument("--threads-per-track", type=int, default=0, choices=[0, 1, 2],
+                    help="threads per track of the headline step (0: tuned)")
+    ap.add_argument("--uneven-events", type=int, default=2000,
+                    help="events of the uneven sample (2000: the config-4 workload; fewer for small profiles)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -635,7 +639,7 @@ def main():
     nev = args.nevts
     # schedule and block size left open: the context applies what p2z_autotune measured
     cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule=args.schedule,
-                          block_threads=args.block)
+                          block_threads=args.block, threads_per_track=args.threads_per_track)
     params = p2z.physics_params(seed=20240601 + rank)
     nb = p2z.num_batches(cfg)
     trk_shape, hit_shape = (nb, p2z.TRK_WORDS, 32), (nb, 20, p2z.HIT_WORDS, 32)
@@ -692,7 +696,8 @@ def main():
                            (tune_head["best_bsize32_aosoa"]["schedule"] if tune_head else "flat")),
               "block_threads": (args.block or (tune_head["best_bsize32_aosoa"]["block_threads"] if tune_head
                                                else 128)),
-              "threads_per_track": tune_head["best_bsize32_aosoa"]["threads_per_track"] if tune_head else 1}
+              "threads_per_track": (args.threads_per_track or
+                                    (tune_head["best_bsize32_aosoa"]["threads_per_track"] if tune_head else 1))}
     ref_gpu = None
     if rank == 0 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(p2z, ctx, dt, dh, stream, launch)
@@ -746,7 +751,7 @@ def main():
     # batched (persistent + graph) vs plain (one launch per event) on uneven events
     bvp = None
     if not args.no_uneven:
-        counts = uneven_counts(2000, 77 + rank)
+        counts = uneven_counts(args.uneven_events, 77 + rank)
         ucfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20)
         unb = p2z.num_batches(ucfg)
         udt = torch.empty((unb, p2z.TRK_WORDS, 32), dtype=torch.float32, device="cuda")
@@ -811,7 +816,7 @@ def main():
         back = torch.empty_like(uo.permute(0, 2, 1).reshape(perm.numel(), -1))
         back[perm] = uo.permute(0, 2, 1).reshape(perm.numel(), -1)
         same = bool((back.view(torch.int32) == udo.permute(0, 2, 1).reshape(perm.numel(), -1).view(torch.int32)).all())
-        bvp = {"workload": "2000 events, track counts log-normal (median 3000, sigma 1, clipped 50-30000), "
+        bvp = {"workload": f"{len(counts)} events, track counts log-normal (median 3000, sigma 1, clipped 50-30000), "
                            "5-20 hits/track, 10% layers dropped",
                "tracks": int(counts.sum()), "updates_per_step": u_upd,
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
