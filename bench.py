@@ -450,8 +450,11 @@ def run_serving(p2z, device, rank, args):
 
 def workload_config(nev, world):
     """The workload's description, identical in both arms."""
-    return {"workload": WORKLOAD, "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
-            "updates_per_step_per_gpu": nev * 9600 * 20, "l2": "inputs 8.1 GB > L2, no flush",
+    gb = nev * 9600 * (28 + 20 * 9) * 4 / 1e9
+    return {"workload": WORKLOAD if nev == 1000 else WORKLOAD.replace("1000 events", f"{nev} events"),
+            "events": nev, "tracks_per_event": 9600, "nlayer": 20, "bsize": 32,
+            "updates_per_step_per_gpu": nev * 9600 * 20,
+            "l2": f"inputs {gb:.1f} GB {'>' if gb > 0.126 else '<'} L2, no flush",
             "parallelism": f"dp{world} (independent event shards)"}
 
 
