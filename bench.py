@@ -619,6 +619,8 @@ def main():
     ap.add_argument("--block", type=int, default=0, help="threads per CTA of the headline step (0: tuned)")
     ap.add_argument("--threads-per-track", type=int, default=0, choices=[0, 1, 2],
                     help="threads per track of the headline step (0: tuned)")
+    ap.add_argument("--update", default="v2", choices=["v2", "v2_comp", "3x3_f64", "3x3_comp", "f64"],
+                    help="update kind of the headline step (v2: the precise 2-D form; the others for profiles)")
     ap.add_argument("--uneven-events", type=int, default=2000,
                     help="events of the uneven sample (2000: the config-4 workload; fewer for small profiles)")
     args = ap.parse_args()
@@ -642,7 +644,7 @@ def main():
     nev = args.nevts
     # schedule and block size left open: the context applies what p2z_autotune measured
     cfg = p2z.make_config(bsize=32, nevts=nev, ntrks=9600, nlayer=20, schedule=args.schedule,
-                          block_threads=args.block, threads_per_track=args.threads_per_track)
+                          block_threads=args.block, threads_per_track=args.threads_per_track, update=args.update)
     params = p2z.physics_params(seed=20240601 + rank)
     nb = p2z.num_batches(cfg)
     trk_shape, hit_shape = (nb, p2z.TRK_WORDS, 32), (nb, 20, p2z.HIT_WORDS, 32)
@@ -873,7 +875,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(nev, world),
-        "form": "precise (default; no FP64 instruction)",
+        "form": ("precise (default; no FP64 instruction)" if args.update == "v2" else f"update kind {args.update}"),
         "launch": launch,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
