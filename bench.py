@@ -840,7 +840,13 @@ def main():
                    "hbm_frac": (BYTES_HIT_PER_UPDATE * res["persistent"] +
                                 BYTES_TRACK * int(counts.sum()) * res["persistent"] / u_upd) / 1e9 /
                                measured_peaks()["hbm_gbs"],
-                   "note": "present-hit updates; bytes = 24 per present hit + 228 per real track (in, out, mask)"},
+                   "fp32_frac_reference_form": {
+                       k: FLOPS_PER_UPDATE_REFERENCE_FORM * v / 1e12 / fp32_peak_live
+                       for k, v in (("stored_order", res["persistent"]),
+                                    ("sorted_windows", res["persistent_sorted_windows"]),
+                                    ("ordered_by_hits", ordered["persistent"]))},
+                   "note": "present-hit updates; bytes = 24 per present hit + 228 per real track (in, out, mask); "
+                           "fp32_frac_reference_form counts the update as the reference writes it"},
                "block_threads": blocks,
                "ordered_by_hits": {"note": "same events, each event's tracks packed in order of hit count",
                                    "batched_persistent_graph": ordered["persistent"],
