@@ -334,6 +334,11 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   spec.block = pl.block;
   spec.grid = 0;
   spec.tpt = pl.tpt;
+  // Launches of at most 4 warps per SM leave each scheduler about one warp, with
+  // nothing to run while it waits for a layer's hits from DRAM: those launches
+  // ask L2 for their batches' hit blocks first (AOSOA).
+  const int64_t small_slots = (int64_t)ctx->num_sms * 4 * 32 / pl.tpt;
+  auto prefetch_for = [&](int64_t n) { return (!pl.soa && n <= small_slots) ? 1 : 0; };
   if (pl.tpt != 1 && schedule == P2Z_SCHED_STAGED)
     return fail(ctx, P2Z_UNSUPPORTED, "the staged schedule has one thread per track");
   if (schedule == P2Z_SCHED_PER_EVENT) {
@@ -352,6 +357,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
       if (b <= a) continue;
       spec.args.slot_begin = a;
       spec.args.slot_end = b;
+      spec.args.l2_prefetch = prefetch_for(b - a);
       P2Z_CUDA(ctx, dispatch(spec, spread ? ctx->ev_streams[k++ % kEventStreams] : st));
       ++*launches;
     }
@@ -366,6 +372,7 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
   spec.args.slot_begin = s0;
   spec.args.slot_end = s1;
   if (s1 <= s0) return P2Z_OK;
+  spec.args.l2_prefetch = prefetch_for(s1 - s0);  // (the staged kernel stages its hits itself)
   // masked flat and persistent runs: process each window's slots in order of hit count
   const bool sort = spec.masked && (pl.flags & P2Z_FLAG_SORT_WINDOWS) &&
                     (schedule == P2Z_SCHED_FLAT || schedule == P2Z_SCHED_PERSISTENT);

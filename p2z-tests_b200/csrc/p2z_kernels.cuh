@@ -80,6 +80,10 @@ struct RunArgs {
   // slot window_base(s) + perm[s].  perm == nullptr: s itself.
   const uint8_t *__restrict__ perm;
   int win;                         // slots per window, a power of two <= 256
+  // 1: each thread first asks L2 for its batch's whole hit block (AOSOA), so
+  // that a launch too small to fill the GPU -- whose warps have no others to
+  // hide a layer's DRAM latency behind -- waits on L2 instead (set by the host).
+  int l2_prefetch;
 };
 
 // The slot a thread processes (see RunArgs::perm).
@@ -113,6 +117,20 @@ __device__ __forceinline__ const float *hit_lane(const float *hits, int64_t slot
     const int t = (int)(slot % B);
     return hits + (b * nlayer + l) * (int64_t)(HIT_WORDS * B) + t;
   }
+}
+
+// Requests the hit block of slot's batch into L2: its nlayer layers are
+// contiguous, nlayer * 9 * B words; the batch's B lanes share the block's
+// 128-byte pieces, lane t taking pieces t, t + B, ...  Every address is inside
+// the block.
+template <int B>
+__device__ __forceinline__ void prefetch_hits_l2(const float *hits, int64_t slot, int nlayer) {
+  static_assert(B > 0, "AOSOA only");
+  const int64_t b = slot / B;
+  const int t = (int)(slot % B);
+  const int bytes = nlayer * HIT_WORDS * B * 4;
+  const char *base = reinterpret_cast<const char *>(hits + b * (int64_t)nlayer * HIT_WORDS * B);
+  for (int off = t * 128; off < bytes; off += B * 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + off));
 }
 
 // Hit words a kernel needs: x, y, z, V00, V10, V11 and, for the 3-D update,
@@ -204,6 +222,9 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
   const bool writer = TPT == 1 || !ln.j;
   const uint32_t all = (a.nlayer >= 32) ? 0xffffffffu : ((1u << a.nlayer) - 1u);
   uint32_t m = MASKED ? (__ldg(a.mask + slot) & all) : all;
+  if constexpr (B > 0) {
+    if (a.l2_prefetch && m != 0u) prefetch_hits_l2<B>(a.hits, slot, a.nlayer);
+  }
 
   float in[TRK_WORDS];
 #pragma unroll

@@ -226,6 +226,8 @@ void launch_group(p2z_server *s) {
     }
     spec.args.slot_begin = b_begin * B;
     spec.args.slot_end = b_end * B;
+    // a run of at most 4 warps per SM asks L2 for its hit blocks first (as p2z_run_device)
+    spec.args.l2_prefetch = (spec.args.slot_end - spec.args.slot_begin) <= (int64_t)s->num_sms * 4 * 32 ? 1 : 0;
     const int64_t items = (spec.args.slot_end - spec.args.slot_begin + 31) / 32;
     spec.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)occ * s->num_sms, (items * 32 + spec.block - 1) /
                                                                                               spec.block));
