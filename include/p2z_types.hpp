@@ -358,6 +358,10 @@ struct RunOptions {
   p2z_update_kind update = P2Z_UPDATE_V2;
   uint32_t flags = 0;  /* P2Z_FLAG_*, e.g. P2Z_FLAG_REFERENCE_ROUNDING */
   float kfact = 0.f;
+  /* launch shape; 0 / AUTO: what p2z_autotune measured best on the device, else the defaults */
+  p2z_schedule schedule = P2Z_SCHED_AUTO;
+  int block_threads = 0;
+  int threads_per_track = 0;
 };
 
 /* The reference's timed loop (:731-748) -- for every event, batch and layer,
@@ -377,6 +381,9 @@ p2z_stats run(const Device &dev, const ALLTRKS<B> &trk, const ALLHITS<B> &hit, A
   c.kfact = o.kfact;
   c.update = o.update;
   c.flags = o.flags;
+  c.schedule = o.schedule;
+  c.block_threads = o.block_threads;
+  c.threads_per_track = o.threads_per_track;
   p2z_stats st{};
   check(p2z_run(dev.get(), &c, trk.btrks, hit.bhits, nullptr, out.btrks, &st), dev.get());
   return st;
