@@ -655,10 +655,10 @@ def main():
     ctx.generate_physics_device(cfg, dt, dh, params=params)
     updates = nev * 9600 * 20
     do = torch.empty_like(dt)
-    # host copy of the first events for the CPU baseline (rank 0)
+    # host copy of the first events for the CPU baseline (one GPU only: it measures the host's cores)
     n_cpu_ev = cpu_sample_events(os.cpu_count() or 1)
     cpu_sample = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         cpu_sample = (dt[:n_cpu_ev * 300].cpu().numpy(), dh[:n_cpu_ev * 300].cpu().numpy())
 
     def step(c=cfg):
