@@ -307,17 +307,19 @@ __device__ __forceinline__ void process_slot(const RunArgs &a, int64_t slot) {
     if (l < nl) singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
   } else {
     // present layers in order: lowest set bit first
+    const int64_t stride = HIT_WORDS * WS;
+    const float *hp = hit_lane<B>(a.hits, slot, a.nlayer, 0, WS);
     uint32_t rest = m & (m - 1u);
-    load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(m) - 1, WS), WS);
-    if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
+    load_hit<NH>(h0, hp + (__ffs(m) - 1) * stride, WS);
+    if (rest) load_hit<NH>(h1, hp + (__ffs(rest) - 1) * stride, WS);
     singular |= step<UPD, SC, true, TPT>(s, b21, h0, k, ik, ln);
     while (rest) {
       rest &= rest - 1u;  // h1 holds the layer just removed from rest
-      if (rest) load_hit<NH>(h0, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
+      if (rest) load_hit<NH>(h0, hp + (__ffs(rest) - 1) * stride, WS);
       singular |= step<UPD, SC, false, TPT>(s, b21, h1, k, ik, ln);
       if (!rest) break;
       rest &= rest - 1u;  // h0 holds the layer just removed
-      if (rest) load_hit<NH>(h1, hit_lane<B>(a.hits, slot, a.nlayer, __ffs(rest) - 1, WS), WS);
+      if (rest) load_hit<NH>(h1, hp + (__ffs(rest) - 1) * stride, WS);
       singular |= step<UPD, SC, false, TPT>(s, b21, h0, k, ik, ln);
     }
   }
