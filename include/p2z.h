@@ -317,6 +317,26 @@ p2z_status p2z_relayout_device(p2z_context *ctx, const p2z_config *from, const p
                                const void *d_trk_in, const void *d_hits_in, const uint32_t *d_mask_in,
                                void *d_trk_out, void *d_hits_out, uint32_t *d_mask_out, void *stream);
 
+/* Packing tracks with missing layers in order of hit count.  A warp's 32
+ * tracks take as many steps as the one with the most hits, so an uneven
+ * sample runs fastest when each batch holds tracks of similar hit counts.
+ * p2z_pack_by_hits_device writes a copy of cfg's AOSOA arrays (tracks, hits
+ * and, when given, masks) in which every event's tracks are in order of
+ * decreasing hit count -- a stable order: equal counts keep their order; every
+ * event keeps its own slots and its padding last -- and d_perm[s] = the input
+ * slot that packed slot s holds (int64 per slot, nbatches * bsize of them).
+ * Runs on the packed arrays give each track the bits it gets in the caller's
+ * order; p2z_unpack_tracks_device writes a packed output back in the caller's
+ * order.  No mask: every track has every layer and the order is unchanged.
+ * The copies must not alias the inputs.  Pack: synchronous (it allocates
+ * scratch for the sort); unpack: enqueued on `stream` (NULL = the context's).
+ * No counterpart in the reference. */
+p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in,
+                                   const void *d_hits_in, const uint32_t *d_mask_in, void *d_trk_out,
+                                   void *d_hits_out, uint32_t *d_mask_out, int64_t *d_perm, void *stream);
+p2z_status p2z_unpack_tracks_device(p2z_context *ctx, const p2z_config *cfg, const int64_t *d_perm,
+                                    const void *d_trk_packed, void *d_trk_out, void *stream);
+
 /* One measured launch configuration. */
 typedef struct p2z_tune_entry {
   int32_t bsize;          /* 8, 16, 32, 64 */

@@ -205,6 +205,8 @@ _SIGS = {
                                     C.POINTER(C.c_double), C.POINTER(RequestInfo)]),
     "p2z_relayout_device": (C.c_int, [_VP, C.POINTER(Config), C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP, _VP,
                                       _VP]),
+    "p2z_pack_by_hits_device": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, _VP, _VP, _VP, _VP, _VP]),
+    "p2z_unpack_tracks_device": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _VP, _VP]),
     "p2z_autotune": (C.c_int, [_VP, C.POINTER(Config), _CVP, _CVP, _CVP, C.c_int, C.POINTER(TuneEntry), C.c_int,
                                C.POINTER(C.c_int), C.POINTER(TuneEntry)]),
     "p2z_measure_peaks": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(Peaks)]),
@@ -620,6 +622,21 @@ class Context:
         _check(lib.p2z_relayout_device(self.h, C.byref(cfg_from), C.byref(cfg_to), _ptr(d_trk_in), _ptr(d_hits_in),
                                        _ptr(d_mask_in), _ptr(d_trk_out), _ptr(d_hits_out), _ptr(d_mask_out),
                                        stream), self.h)
+
+    def pack_by_hits_device(self, cfg: Config, d_trk_in, d_hits_in, d_trk_out, d_hits_out, d_perm,
+                            d_mask_in=None, d_mask_out=None, stream=None):
+        """Copy of the arrays with every event's tracks in order of decreasing hit
+        count, and d_perm[s] = the input slot of packed slot s (p2z_pack_by_hits_device)."""
+        stream = _stream(stream, d_trk_in, d_hits_in, d_mask_in, d_trk_out, d_hits_out, d_mask_out, d_perm)
+        _check(lib.p2z_pack_by_hits_device(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits_in), _ptr(d_mask_in),
+                                           _ptr(d_trk_out), _ptr(d_hits_out), _ptr(d_mask_out), _ptr(d_perm),
+                                           stream), self.h)
+
+    def unpack_tracks_device(self, cfg: Config, d_perm, d_trk_packed, d_trk_out, stream=None):
+        """A packed run's output back in the caller's slot order (p2z_unpack_tracks_device)."""
+        stream = _stream(stream, d_perm, d_trk_packed, d_trk_out)
+        _check(lib.p2z_unpack_tracks_device(self.h, C.byref(cfg), _ptr(d_perm), _ptr(d_trk_packed), _ptr(d_trk_out),
+                                            stream), self.h)
 
     def autotune(self, cfg: Config, d_trk_in, d_hits, d_mask=None, reps=3, max_entries=256):
         """Measure every bsize x layout x schedule x block size (p2z_autotune).
