@@ -328,8 +328,9 @@ p2z_status p2z_relayout_device(p2z_context *ctx, const p2z_config *from, const p
  * Runs on the packed arrays give each track the bits it gets in the caller's
  * order; p2z_unpack_tracks_device writes a packed output back in the caller's
  * order.  No mask: every track has every layer and the order is unchanged.
- * The copies must not alias the inputs.  Pack: synchronous (it allocates
- * scratch for the sort); unpack: enqueued on `stream` (NULL = the context's).
+ * The copies must not alias the inputs.  Pack: synchronous (its scratch, about
+ * 32 bytes a slot, is the context's reusable device buffer); unpack: enqueued
+ * on `stream` (NULL = the context's).
  * No counterpart in the reference. */
 p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in,
                                    const void *d_hits_in, const uint32_t *d_mask_in, void *d_trk_out,

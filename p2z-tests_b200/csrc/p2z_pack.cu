@@ -23,6 +23,7 @@ void set_context_free_error(const char *msg);
 int context_device(const p2z_context *ctx);
 cudaStream_t context_stream(const p2z_context *ctx);
 p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg);
+void *context_scratch(p2z_context *ctx, size_t bytes);
 }  // namespace p2z
 
 using namespace p2z;
@@ -40,21 +41,7 @@ namespace {
     }                                                                                           \
   } while (0)
 
-// Device buffers freed on scope exit.
-struct Scratch {
-  std::vector<void *> p;
-  ~Scratch() {
-    for (void *q : p)
-      if (q) cudaFree(q);
-  }
-  cudaError_t alloc(void **out, size_t bytes) {
-    *out = nullptr;
-    if (bytes == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(out, bytes);
-    if (e == cudaSuccess) p.push_back(*out);
-    return e;
-  }
-};
+size_t up256(size_t n) { return (n + 255) / 256 * 256; }
 
 // Sort key of slot s: (event << 6) | rank class, where the class is
 // 32 - (hit count) for a real track (0: every one of 32 layers present) and
@@ -152,12 +139,19 @@ p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, cons
   std::vector<int64_t> counts, beg;
   event_tables(cfg, counts, beg);
   const int ne = (int)cfg->nevts;
-  Scratch scr;
-  void *tab = nullptr, *keys = nullptr, *keys_sorted = nullptr, *idx = nullptr, *tmp = nullptr;
-  PACK_CUDA(ctx, scr.alloc(&tab, sizeof(int64_t) * (2 * (size_t)ne + 1)));
-  PACK_CUDA(ctx, scr.alloc(&keys, sizeof(uint64_t) * (size_t)ns));
-  PACK_CUDA(ctx, scr.alloc(&keys_sorted, sizeof(uint64_t) * (size_t)ns));
-  PACK_CUDA(ctx, scr.alloc(&idx, sizeof(int64_t) * (size_t)ns));
+  // the sort's bits: 6 for the class, then the event index
+  int end_bit = 6;
+  while (end_bit < 64 && ((uint64_t)ne - 1) >> (end_bit - 6)) ++end_bit;
+  size_t tmp_bytes = 0;
+  PACK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                                 (const int64_t *)nullptr, (int64_t *)nullptr, ns, 0, end_bit, st));
+  // scratch, from the context's reusable device buffer (parts 256-byte aligned): event tables,
+  // keys, sorted keys, slot indices, the sort's temporary storage
+  const size_t b_tab = up256(sizeof(int64_t) * (2 * (size_t)ne + 1)), b_keys = up256(sizeof(uint64_t) * (size_t)ns);
+  char *scr = static_cast<char *>(context_scratch(ctx, b_tab + 3 * b_keys + up256(tmp_bytes)));
+  if (!scr) return context_fail(ctx, P2Z_OOM, "no device memory for the packing scratch");
+  void *tab = scr, *keys = scr + b_tab, *keys_sorted = scr + b_tab + b_keys, *idx = scr + b_tab + 2 * b_keys;
+  void *tmp = scr + b_tab + 3 * b_keys;
   int64_t *d_counts = (int64_t *)tab, *d_beg = d_counts + ne;
   PACK_CUDA(ctx, cudaMemcpyAsync(d_counts, counts.data(), sizeof(int64_t) * ne, cudaMemcpyHostToDevice, st));
   PACK_CUDA(ctx, cudaMemcpyAsync(d_beg, beg.data(), sizeof(int64_t) * (ne + 1), cudaMemcpyHostToDevice, st));
@@ -166,12 +160,6 @@ p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, cons
   k_pack_keys<<<gx, 256, 0, st>>>(d_mask_in, d_beg, d_counts, ne, ns, all, (uint64_t *)keys, (int64_t *)idx);
   PACK_CUDA(ctx, cudaGetLastError());
   // stable radix sort of (event, class) over the bits the keys use
-  int end_bit = 6;
-  while (end_bit < 64 && ((uint64_t)ne - 1) >> (end_bit - 6)) ++end_bit;
-  size_t tmp_bytes = 0;
-  PACK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (const uint64_t *)keys, (uint64_t *)keys_sorted,
-                                                 (const int64_t *)idx, d_perm, ns, 0, end_bit, st));
-  PACK_CUDA(ctx, scr.alloc(&tmp, tmp_bytes));
   PACK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, (const uint64_t *)keys, (uint64_t *)keys_sorted,
                                                  (const int64_t *)idx, d_perm, ns, 0, end_bit, st));
   const int B = cfg->bsize, nl = cfg->nlayer;
