@@ -738,7 +738,7 @@ def main():
         e2e = {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s",
                "h2d_bytes_per_step": int(s.h2d_bytes), "d2h_bytes_per_step": int(s.d2h_bytes),
                "ms_per_step": e2e_ms, "steps": n_e2e,
-               "path": "p2z_run, pinned host buffers, 8 chunks on 2 streams (copy/compute overlap)",
+               "path": "p2z_run, pinned host buffers, 16 chunks on 2 streams (copy/compute overlap)",
                "roofline": {"bound": "host link (PCIe)", "link_floor_ms": link_ms, "frac": link_ms / e2e_ms,
                             "ceiling_updates_per_s": updates * world / (link_ms / 1e3),
                             "peaks": {k: live_peaks[k] for k in ("h2d_gbs", "d2h_gbs", "bidir_gbs")},

@@ -236,7 +236,7 @@ size_t p2z_sizeof_mphit(int bsize);   /* 9*bsize*4 */
  *   trk_out  MPTRK[nbatches]            (host; may equal trk_in)
  * Host buffers that are page-locked (cudaHostAlloc / p2z_host_alloc) are
  * copied asynchronously; pageable ones go through a staging path.  The work is
- * split into up to 8 chunks whose copies and passes alternate between two
+ * split into up to 16 chunks whose copies and passes alternate between two
  * streams.  With page-locked buffers (all of trk_in, hits, trk_out and
  * hit_mask when given) the whole pipeline is recorded as a CUDA graph on the
  * first call and replayed by later calls with the same config, host buffers

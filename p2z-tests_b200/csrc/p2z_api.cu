@@ -15,9 +15,10 @@
 #include "p2z_kernels.cuh"
 
 // p2z_run: the host<->device copies and the kernels are pipelined over at most
-// this many chunks (alternating between two streams).
+// this many chunks (alternating between two streams).  Measured on one B200 for
+// the 1000-event sample: 8 chunks 108.4 ms, 16 107.8 ms, 32 108.1-108.5 ms.
 #ifndef P2Z_RUN_MAX_CHUNKS
-#define P2Z_RUN_MAX_CHUNKS 8
+#define P2Z_RUN_MAX_CHUNKS 16
 #endif
 // P2Z_FLAG_PER_EVENT_STREAMS: streams the per-event launches are spread over.
 constexpr int kEventStreams = 10;
@@ -866,7 +867,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
   // With page-locked host buffers the pipeline is recorded once as a CUDA
   // graph and replayed while the plan and every buffer it touches stay the
   // same: a call then costs one graph launch instead of enqueueing each copy
-  // and kernel (8 chunks x 4-5 operations, or one launch per event).
+  // and kernel (16 chunks x 4-5 operations, or one launch per event).
   // Pageable buffers are copied through the driver's staging path, which a
   // graph cannot hold, so they take the direct path, as does P2Z_FLAG_NO_GRAPH.
   const bool graph = !(pl.flags & P2Z_FLAG_NO_GRAPH) && pl.nslots > 0 && page_locked(trk_in) && page_locked(hits) &&
