@@ -60,8 +60,13 @@ struct Types {
   // Register budget: kernels allow up to 256 threads per CTA and ask ptxas
   // for MIN_CTAS such CTAs per SM.  For the 2-D FP32 kinds, 3 caps them at 80
   // registers (24 resident warps per SM), which measured faster than the 88
-  // ptxas picks unconstrained; 1 leaves the count to ptxas.
-  static constexpr int MIN_CTAS = (UPD == UPDK_V2 || UPD == UPDK_V2_COMP) ? 3 : 1;
+  // ptxas picks unconstrained.  For the 3x3 update with its FP64 island, 2
+  // caps it at 128 (16 warps instead of the 12 that 157-164 registers allow;
+  // with the Joseph form evaluated a row at a time the cap spills 4 bytes):
+  // 4.44 against 4.51 ms on the headline sample, 4.32 against 5.63 ms on the
+  // masked uneven one (persistent).  1 leaves the count to ptxas.
+  static constexpr int MIN_CTAS =
+      (UPD == UPDK_V2 || UPD == UPDK_V2_COMP) ? 3 : (UPD == UPDK_3X3_F64 ? 2 : 1);
 };
 
 struct RunArgs {

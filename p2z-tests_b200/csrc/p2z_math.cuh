@@ -942,9 +942,11 @@ __device__ __forceinline__ float cof2<float>(float a, float b, float c, float d)
 template <typename U, typename A>
 __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float (&hp)[3], const float (&hv)[6]) {
   const U v00 = hv[0], v10 = hv[1], v11 = hv[2], v20 = hv[3], v21 = hv[4], v22 = hv[5];
-  const U C00 = s.c00, C10 = s.c10, C11 = s.c11, C30 = s.c30, C31 = s.c31, C33 = s.c33;
-  const U C40 = s.c40, C41 = s.c41, C43 = s.c43, C44 = s.c44;
-  const U C50 = s.c50, C51 = s.c51, C53 = s.c53, C54 = s.c54, C55 = s.c55;
+  // C's live elements as they enter the update, in float (converted where used)
+  const float f00 = s.c00, f10 = s.c10, f11 = s.c11, f30 = s.c30, f31 = s.c31, f33 = s.c33;
+  const float f40 = s.c40, f41 = s.c41, f43 = s.c43, f44 = s.c44;
+  const float f50 = s.c50, f51 = s.c51, f53 = s.c53, f54 = s.c54, f55 = s.c55;
+  const U C00 = f00, C10 = f10, C11 = f11, C30 = f30, C31 = f31, C40 = f40, C41 = f41, C50 = f50, C51 = f51;
   const U R00 = C00 + v00, R10 = C10 + v10, R11 = C11 + v11, R20 = v20, R21 = v21, R22 = v22;
   // cofactors of the symmetric R; cof2(a, b, c, d) = a*d - b*c
   const U A00 = cof2<U>(R11, R21, R21, R22);  // R11*R22 - R21*R21
@@ -980,33 +982,33 @@ __device__ __forceinline__ bool update_3x3_joseph(Trk<float, A> &s, const float 
   // - K(i,1) C(1,j) (C(2,j) = 0) and P(i,2) = 0, so E(i,m) = P(i,m) - (K V)(i,m)
   // for m = x, y and E(i,z) = -(K V)(i,z).  Three products per element of C''
   // instead of the five of P - P H^T K^T + K V K^T.
-  const U Cm[5][5] = {{C00, C10, C30, C40, C50},
-                      {C10, C11, C31, C41, C51},
-                      {C30, C31, C33, C43, C53},
-                      {C40, C41, C43, C44, C54},
-                      {C50, C51, C53, C54, C55}};
-  U P[5][5];
-#pragma unroll
-  for (int i = 0; i < 5; ++i)
-#pragma unroll
-    for (int j = 0; j < 5; ++j) P[i][j] = Cm[i][j] - (K[i][0] * Cm[0][j] + K[i][1] * Cm[1][j]);
-  U E[5][3];
+  // One row of C'' at a time (rows x, y, ipt, phi, theta of the live 5x5
+  // block), so that only the gain, C's rows x and y (the measured columns, kept
+  // as they were) and the current row are live: C'' is written into the track
+  // as each row is finished.
+  const float Cr0[5] = {f00, f10, f30, f40, f50};  // C(0, j)
+  const float Cr1[5] = {f10, f11, f31, f41, f51};  // C(1, j)
+  float *const out[5][5] = {{&s.c00, nullptr, nullptr, nullptr, nullptr},
+                            {&s.c10, &s.c11, nullptr, nullptr, nullptr},
+                            {&s.c30, &s.c31, &s.c33, nullptr, nullptr},
+                            {&s.c40, &s.c41, &s.c43, &s.c44, nullptr},
+                            {&s.c50, &s.c51, &s.c53, &s.c54, &s.c55}};
+  const float Crow[5][5] = {{f00, f10, f30, f40, f50},
+                            {f10, f11, f31, f41, f51},
+                            {f30, f31, f33, f43, f53},
+                            {f40, f41, f43, f44, f54},
+                            {f50, f51, f53, f54, f55}};
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
-    E[i][0] = P[i][0] - (K[i][0] * v00 + K[i][1] * v10 + K[i][2] * v20);
-    E[i][1] = P[i][1] - (K[i][0] * v10 + K[i][1] * v11 + K[i][2] * v21);
-    E[i][2] = -(K[i][0] * v20 + K[i][1] * v21 + K[i][2] * v22);
+    U P[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) P[j] = U(Crow[i][j]) - (K[i][0] * U(Cr0[j]) + K[i][1] * U(Cr1[j]));
+    const U E0 = P[0] - (K[i][0] * v00 + K[i][1] * v10 + K[i][2] * v20);
+    const U E1 = P[1] - (K[i][0] * v10 + K[i][1] * v11 + K[i][2] * v21);
+    const U E2 = -(K[i][0] * v20 + K[i][1] * v21 + K[i][2] * v22);
+#pragma unroll
+    for (int j = 0; j <= i; ++j) *out[i][j] = float(P[j] - (E0 * K[j][0] + E1 * K[j][1] + E2 * K[j][2]));
   }
-  U N[5][5];
-#pragma unroll
-  for (int i = 0; i < 5; ++i)
-#pragma unroll
-    for (int j = 0; j <= i; ++j) N[i][j] = P[i][j] - (E[i][0] * K[j][0] + E[i][1] * K[j][1] + E[i][2] * K[j][2]);
-  s.c00 = float(N[0][0]); s.c10 = float(N[1][0]); s.c11 = float(N[1][1]);
-  s.c30 = float(N[2][0]); s.c31 = float(N[2][1]); s.c33 = float(N[2][2]);
-  s.c40 = float(N[3][0]); s.c41 = float(N[3][1]); s.c43 = float(N[3][2]); s.c44 = float(N[3][3]);
-  s.c50 = float(N[4][0]); s.c51 = float(N[4][1]); s.c53 = float(N[4][2]); s.c54 = float(N[4][3]);
-  s.c55 = float(N[4][4]);
   return !(det > U(0));
 }
 
