@@ -825,7 +825,7 @@ def main():
         # run on the packed copy and p2z_unpack_tracks_device puts each output back in the caller's order
         del back
         pt_, ph_, pm_ = torch.empty_like(udt), torch.empty_like(udh), torch.empty_like(udm)
-        pperm = torch.empty(unb * 32, dtype=torch.int64, device="cuda")
+        pperm = torch.empty(2 * unb * 32, dtype=torch.int64, device="cuda")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.pack_by_hits_device(ucfg, udt, udh, pt_, ph_, pperm, d_mask_in=udm, d_mask_out=pm_, stream=stream)

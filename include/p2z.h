@@ -323,8 +323,10 @@ p2z_status p2z_relayout_device(p2z_context *ctx, const p2z_config *from, const p
  * p2z_pack_by_hits_device writes a copy of cfg's AOSOA arrays (tracks, hits
  * and, when given, masks) in which every event's tracks are in order of
  * decreasing hit count -- a stable order: equal counts keep their order; every
- * event keeps its own slots and its padding last -- and d_perm[s] = the input
- * slot that packed slot s holds (int64 per slot, nbatches * bsize of them).
+ * event keeps its own slots and its padding last -- and the permutation in
+ * d_perm, 2 * nbatches * bsize int64: d_perm[s] = the input slot that packed
+ * slot s holds, and after those the inverse, d_perm[nslots + q] = the packed
+ * slot of input slot q.
  * Runs on the packed arrays give each track the bits it gets in the caller's
  * order; p2z_unpack_tracks_device writes a packed output back in the caller's
  * order.  No mask: every track has every layer and the order is unchanged.

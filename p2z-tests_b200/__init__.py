@@ -626,7 +626,8 @@ class Context:
     def pack_by_hits_device(self, cfg: Config, d_trk_in, d_hits_in, d_trk_out, d_hits_out, d_perm,
                             d_mask_in=None, d_mask_out=None, stream=None):
         """Copy of the arrays with every event's tracks in order of decreasing hit
-        count, and d_perm[s] = the input slot of packed slot s (p2z_pack_by_hits_device)."""
+        count, and in d_perm (2 x nslots int64) the input slot of every packed slot followed by
+        the inverse (p2z_pack_by_hits_device)."""
         stream = _stream(stream, d_trk_in, d_hits_in, d_mask_in, d_trk_out, d_hits_out, d_mask_out, d_perm)
         _check(lib.p2z_pack_by_hits_device(self.h, C.byref(cfg), _ptr(d_trk_in), _ptr(d_hits_in), _ptr(d_mask_in),
                                            _ptr(d_trk_out), _ptr(d_hits_out), _ptr(d_mask_out), _ptr(d_perm),

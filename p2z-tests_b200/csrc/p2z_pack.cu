@@ -65,24 +65,28 @@ __global__ void k_pack_keys(const uint32_t *__restrict__ mask, const int64_t *__
   idx[s] = s;
 }
 
-// AOSOA word of (slot, row): tracks row = element, hits row = layer * 9 + element.
-__device__ __forceinline__ int64_t aosoa_word(int B, int64_t s, int row, int nlayer, bool hits) {
-  const int64_t b = s / B, t = s % B;
-  if (!hits) return b * (int64_t)(TRK_WORDS * B) + (int64_t)row * B + t;
-  const int l = row / HIT_WORDS, e = row % HIT_WORDS;
-  return (b * nlayer + l) * (int64_t)(HIT_WORDS * B) + (int64_t)e * B + t;
-}
+// One slot's words in an AOSOA array whose batches are `bw` words long (28 B
+// for tracks; nlayer * 9 * B for hits, whose layers of a batch are
+// contiguous): word r of slot s is at (s / B) * bw + s % B + r * B.
+__device__ __forceinline__ int64_t slot_base(int64_t s, int B, int64_t bw) { return (s / B) * bw + s % B; }
 
-// dst slot s (x), row (y): GATHER dst[s] = src[perm[s]], else dst[perm[s]] = src[s].
+// Thread = slot s of the packed order, copying all `rows` words of a slot:
+// GATHER dst[s] = src[perm[s]] (packing), else dst[perm[s]] = src[s] (unpacking).
 template <bool GATHER>
 __global__ void k_permute(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
-                          const int64_t *__restrict__ perm, int64_t nslots, int B, int nlayer, int hits) {
+                          const int64_t *__restrict__ perm, int64_t nslots, int B, int rows, int64_t bw) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots) return;
-  const int row = blockIdx.y;
   const int64_t p = perm[s];
-  if (GATHER) dst[aosoa_word(B, s, row, nlayer, hits)] = src[aosoa_word(B, p, row, nlayer, hits)];
-  else dst[aosoa_word(B, p, row, nlayer, hits)] = src[aosoa_word(B, s, row, nlayer, hits)];
+  const int64_t from = slot_base(GATHER ? p : s, B, bw), to = slot_base(GATHER ? s : p, B, bw);
+#pragma unroll 4
+  for (int r = 0; r < rows; ++r) dst[to + (int64_t)r * B] = src[from + (int64_t)r * B];
+}
+
+// inv[perm[s]] = s
+__global__ void k_invert(const int64_t *__restrict__ perm, int64_t *__restrict__ inv, int64_t nslots) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nslots) inv[perm[s]] = s;
 }
 
 __global__ void k_gather_mask(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
@@ -163,11 +167,12 @@ p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, cons
   PACK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, (const uint64_t *)keys, (uint64_t *)keys_sorted,
                                                  (const int64_t *)idx, d_perm, ns, 0, end_bit, st));
   const int B = cfg->bsize, nl = cfg->nlayer;
-  k_permute<true><<<dim3(gx, TRK_WORDS), 256, 0, st>>>((const uint32_t *)d_trk_in, (uint32_t *)d_trk_out, d_perm, ns,
-                                                      B, nl, 0);
-  k_permute<true><<<dim3(gx, HIT_WORDS * nl), 256, 0, st>>>((const uint32_t *)d_hits_in, (uint32_t *)d_hits_out,
-                                                           d_perm, ns, B, nl, 1);
+  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_trk_in, (uint32_t *)d_trk_out, d_perm, ns, B, TRK_WORDS,
+                                      (int64_t)TRK_WORDS * B);
+  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_hits_in, (uint32_t *)d_hits_out, d_perm, ns, B,
+                                      HIT_WORDS * nl, (int64_t)HIT_WORDS * nl * B);
   if (d_mask_in) k_gather_mask<<<gx, 256, 0, st>>>(d_mask_in, d_mask_out, d_perm, ns);
+  k_invert<<<gx, 256, 0, st>>>(d_perm, d_perm + ns, ns);
   PACK_CUDA(ctx, cudaGetLastError());
   PACK_CUDA(ctx, cudaStreamSynchronize(st));
   return P2Z_OK;
@@ -188,8 +193,9 @@ p2z_status p2z_unpack_tracks_device(p2z_context *ctx, const p2z_config *cfg, con
   PACK_CUDA(ctx, cudaSetDevice(context_device(ctx)));
   cudaStream_t st = stream ? (cudaStream_t)stream : context_stream(ctx);
   const unsigned gx = (unsigned)((ns + 255) / 256);
-  k_permute<false><<<dim3(gx, TRK_WORDS), 256, 0, st>>>((const uint32_t *)d_trk_packed, (uint32_t *)d_trk_out, d_perm,
-                                                       ns, cfg->bsize, cfg->nlayer, 0);
+  // a gather through the inverse permutation (d_perm's second half): the writes are coalesced
+  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_trk_packed, (uint32_t *)d_trk_out, d_perm + ns, ns,
+                                      cfg->bsize, TRK_WORDS, (int64_t)TRK_WORDS * cfg->bsize);
   PACK_CUDA(ctx, cudaGetLastError());
   return P2Z_OK;
 }

@@ -39,11 +39,13 @@ def test_pack_order_words_and_round_trip(p2z, ctx, bsize):
     nb = p2z.num_batches(cfg)
     dt, dh, dm = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda(), torch.from_numpy(m.view(np.int32)).cuda()
     pt, ph, pm = torch.empty_like(dt), torch.empty_like(dh), torch.empty_like(dm)
-    perm = torch.empty(nb * bsize, dtype=torch.int64, device="cuda")
+    perm = torch.empty(2 * nb * bsize, dtype=torch.int64, device="cuda")
     ctx.pack_by_hits_device(cfg, dt, dh, pt, ph, perm, d_mask_in=dm, d_mask_out=pm)
     torch.cuda.synchronize()
-    got = perm.cpu().numpy()
+    both = perm.cpu().numpy()
+    got, inv = both[:nb * bsize], both[nb * bsize:]
     assert np.array_equal(got, _expected_perm(counts, m, bsize, 20))
+    assert np.array_equal(inv[got], np.arange(nb * bsize))  # the second half is the inverse
     # the packed arrays are the input words of those slots
     T = p2z.tracks_to_soa(t)          # [28][nslots]
     H = p2z.hits_to_soa(h)            # [nlayer][9][nslots]
@@ -67,10 +69,10 @@ def test_pack_without_mask_is_identity_and_refusals(p2z, ctx):
     t, h = p2z.generate_physics(cfg)
     dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
     pt, ph = torch.empty_like(dt), torch.empty_like(dh)
-    perm = torch.empty(3 * 640, dtype=torch.int64, device="cuda")
+    perm = torch.empty(2 * 3 * 640, dtype=torch.int64, device="cuda")
     ctx.pack_by_hits_device(cfg, dt, dh, pt, ph, perm)
     torch.cuda.synchronize()
-    assert np.array_equal(perm.cpu().numpy(), np.arange(3 * 640))
+    assert np.array_equal(perm.cpu().numpy(), np.concatenate([np.arange(3 * 640)] * 2))
     assert np.array_equal(pt.cpu().numpy().view(np.uint32), t.view(np.uint32))
     for kw, status in ((dict(d_mask_in=torch.zeros(3 * 640, dtype=torch.int32, device="cuda")), p2z.BAD_ARG),
                        (dict(), p2z.BAD_ARG)):
