@@ -98,7 +98,8 @@ typedef enum p2z_update_kind {
  *  PER_EVENT   one launch per event (the reference's launch-per-chunk form,
  *              src/propagate-toz-test_CUDA_v4.cu:970-986, taken down to one event per launch).
  *  PERSISTENT  one persistent launch (grid = resident CTAs) whose warps take
- *              32-slot work items from a device queue; replayed as a CUDA graph.
+ *              work items of 32 slots (16 with two threads per track) from a
+ *              device queue; replayed as a CUDA graph.
  *  STAGED      the persistent form with each warp's hit tiles streamed through
  *              shared memory by bulk asynchronous copies, several layers ahead,
  *              and the next batch's tracks copied in during the current one.
