@@ -285,7 +285,7 @@ def tune_summary(best, rows, wall_s):
         return min(sel, key=lambda r: r["ms"]) if sel else None
     out = {"configurations": len(rows), "sweep_wall_s": wall_s, "best": best,
            "best_bsize32_aosoa": fastest(lambda r: r["bsize"] == 32 and r["layout"] == "aosoa")}
-    for key in ("bsize", "layout", "schedule", "threads_per_track"):
+    for key in ("bsize", "layout", "schedule", "threads_per_track", "sorted_windows"):
         vals = sorted({r[key] for r in rows}, key=str)
         out[f"best_per_{key}"] = {str(v): {"ms": fastest(lambda r: r[key] == v)["ms"],
                                            "updates_per_s": fastest(lambda r: r[key] == v)["updates_per_s"]}
@@ -800,6 +800,13 @@ def main():
 
         for sched in ("persistent", "per_event"):
             res[sched] = timed(cfg_for(sched), udt, udh, udm, udo)
+        # the launch shape the autotuner chose for this workload (schedule AUTO, block size and threads
+        # per track open: the context applies the sweep's best, window sorting included)
+        tuned_rate = None
+        if tune_uneven is not None:
+            tuned_rate = timed(p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20,
+                                               schedule="auto", block_threads=0, threads_per_track=0),
+                               udt, udh, udm, udo)
         # the same batched run with each 128-slot window in order of hit count (in-library sort)
         csw = cfg_for("persistent")
         csw.flags |= p2z.FLAG_SORT_WINDOWS
@@ -850,6 +857,10 @@ def main():
                "batched_persistent_graph": res["persistent"], "plain_per_event_launch": res["per_event"],
                "plain_per_event_launch_10_streams": res["per_event_10_streams"],
                "batched_persistent_graph_sorted_windows": res["persistent_sorted_windows"],
+               "batched_autotuned": ({"updates_per_s": tuned_rate,
+                                      "shape": {k: tune_uneven["best_bsize32_aosoa"][k] for k in
+                                                ("schedule", "block_threads", "threads_per_track", "sorted_windows")}}
+                                     if tuned_rate else None),
                "lane_utilisation": {"stored_order": util_packed, "sorted_windows": window_util(udm, 128),
                                     "note": "present-hit lane-steps / (32 x warp steps); sorted_windows: each "
                                             "128-slot window in order of hit count (P2Z_FLAG_SORT_WINDOWS)"},

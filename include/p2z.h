@@ -348,6 +348,7 @@ typedef struct p2z_tune_entry {
   int32_t schedule;       /* P2Z_SCHED_FLAT, _PER_EVENT, _PERSISTENT or _STAGED */
   int32_t block_threads;  /* 32 .. 256 */
   int32_t threads_per_track; /* 1 or 2 */
+  uint32_t flags;         /* P2Z_FLAG_SORT_WINDOWS when the row sorted windows, else 0 */
   double ms;              /* mean device time of one pass */
   double updates_per_s;   /* present-hit updates per second */
 } p2z_tune_entry;
@@ -357,7 +358,8 @@ typedef struct p2z_tune_entry {
  * {8,16,32,64} x layout {AOSOA, SOA} x schedule {FLAT, PERSISTENT, PER_EVENT
  * when nevts <= 4096, and STAGED at bsize 32 AOSOA} x block_threads
  * {32,64,128,256} x threads_per_track {1, and 2 where the update kind and
- * schedule have it}, each the mean
+ * schedule have it} x, for masked runs on the FLAT and PERSISTENT schedules,
+ * window sorting {off, P2Z_FLAG_SORT_WINDOWS}, each the mean
  * of `reps` passes (0 -> 3) after one warm-up pass.  The inputs are converted
  * to each candidate's bsize and layout with p2z_relayout_device into scratch
  * buffers the call allocates and frees (about twice the input size); the
@@ -365,9 +367,10 @@ typedef struct p2z_tune_entry {
  * measured in *n_entries, the first max_entries of them in `entries` (may be
  * NULL when max_entries is 0), the fastest in *best.
  * Side effect: for every (bsize, layout) measured, the context remembers the
- * fastest schedule, block size and threads per track, and later runs with
- * block_threads = 0, schedule = AUTO or threads_per_track = 0 and the same
- * update, flags, bsize, layout and masking use them.  A different bsize or layout is a different data layout, which only
+ * fastest schedule, block size, threads per track and window sorting, and
+ * later runs with block_threads = 0, schedule = AUTO or threads_per_track = 0
+ * and the same update, flags, bsize, layout and masking use them (window
+ * sorting when the schedule is AUTO).  A different bsize or layout is a different data layout, which only
  * the caller can adopt (p2z_relayout_device).  Synchronous. */
 p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
                         const uint32_t *d_hit_mask, int reps, p2z_tune_entry *entries, int max_entries,

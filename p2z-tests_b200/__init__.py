@@ -123,12 +123,14 @@ class ValidationPartial(C.Structure):
 
 class TuneEntry(C.Structure):
     _fields_ = [("bsize", C.c_int32), ("layout", C.c_int32), ("schedule", C.c_int32), ("block_threads", C.c_int32),
-                ("threads_per_track", C.c_int32), ("ms", C.c_double), ("updates_per_s", C.c_double)]
+                ("threads_per_track", C.c_int32), ("flags", C.c_uint32), ("ms", C.c_double),
+                ("updates_per_s", C.c_double)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}
         d["layout"] = LAYOUT_LABELS.get(d["layout"], d["layout"])
         d["schedule"] = SCHED_LABELS.get(d["schedule"], d["schedule"])
+        d["sorted_windows"] = bool(d.pop("flags") & FLAG_SORT_WINDOWS)
         return d
 
 

@@ -63,6 +63,7 @@ struct Tuned {
   int upd, sc, B;
   bool soa, masked;
   int block, schedule, tpt;
+  bool sort;  // P2Z_FLAG_SORT_WINDOWS
 };
 
 }  // namespace
@@ -464,8 +465,9 @@ p2z_status enqueue_pass(p2z_context *ctx, const Plan &pl, const RunArgs &base, i
 }
 
 // Applies the autotuner's measurement for this kind of run to the fields the
-// caller left open (block_threads = 0, schedule = AUTO, threads_per_track =
-// 0), then resolves AUTO.  A tuned shape whose schedule the caller overrides
+// caller left open (block_threads = 0, schedule = AUTO -- with the window
+// sorting measured with that schedule --, threads_per_track = 0), then
+// resolves AUTO.  A tuned shape whose schedule the caller overrides
 // with STAGED keeps one thread per track.
 int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool masked) {
   masked = masked || pl.uneven;
@@ -473,7 +475,10 @@ int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool mas
     for (const Tuned &t : ctx->tuned) {
       if (t.upd == pl.upd && t.sc == pl.sc && t.B == pl.B && t.soa == pl.soa && t.masked == masked) {
         if (cfg->block_threads == 0) pl.block = t.block;
-        if (pl.schedule == P2Z_SCHED_AUTO) pl.schedule = t.schedule;
+        if (pl.schedule == P2Z_SCHED_AUTO) {
+          pl.schedule = t.schedule;
+          if (t.sort) pl.flags |= P2Z_FLAG_SORT_WINDOWS;
+        }
         if (cfg->threads_per_track == 0 && pl.schedule != P2Z_SCHED_STAGED) pl.tpt = t.tpt;
         break;
       }
@@ -565,11 +570,12 @@ p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg) { retu
 void *context_scratch(p2z_context *ctx, size_t bytes) {
   return ensure(ctx, ctx->aux, bytes) == P2Z_OK ? ctx->aux.p : nullptr;
 }
-p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt) {
+p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt,
+                        bool sort) {
   Plan pl;
   p2z_status r = make_plan(ctx, cfg, pl);
   if (r != P2Z_OK) return r;
-  Tuned t{pl.upd, pl.sc, pl.B, pl.soa, masked || pl.uneven, block, schedule, tpt};
+  Tuned t{pl.upd, pl.sc, pl.B, pl.soa, masked || pl.uneven, block, schedule, tpt, sort};
   for (Tuned &o : ctx->tuned) {
     if (o.upd == t.upd && o.sc == t.sc && o.B == t.B && o.soa == t.soa && o.masked == t.masked) {
       o = t;

@@ -19,7 +19,8 @@ void set_context_free_error(const char *msg);
 int context_device(const p2z_context *ctx);
 cudaStream_t context_stream(const p2z_context *ctx);
 p2z_status context_fail(p2z_context *ctx, p2z_status st, const char *msg);
-p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt);
+p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, int block, int schedule, int tpt,
+                        bool sort);
 }  // namespace p2z
 
 using namespace p2z;
@@ -257,18 +258,22 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
       p2z_tune_entry local;
       std::memset(&local, 0, sizeof local);
       local.ms = -1.0;
-      // every (schedule, threads per track, block size) of this bsize and layout
+      // every (schedule, threads per track, window sorting, block size) of this bsize and layout;
+      // window sorting applies to masked runs on the flat and persistent schedules
       struct Shape {
-        int sched, tpt, block;
+        int sched, tpt, sort, block;
       };
       std::vector<Shape> shapes;
       for (int sched : sch)
         for (int tpt = 1; tpt <= ((pair_ok && sched != P2Z_SCHED_STAGED) ? 2 : 1); ++tpt)
-          for (int block : kBlock) shapes.push_back({sched, tpt, block});
+          for (int sort = 0;
+               sort <= ((masked && (sched == P2Z_SCHED_FLAT || sched == P2Z_SCHED_PERSISTENT)) ? 1 : 0); ++sort)
+            for (int block : kBlock) shapes.push_back({sched, tpt, sort, block});
       for (const Shape &sh : shapes) {
         c.schedule = sh.sched;
         c.block_threads = sh.block;
         c.threads_per_track = sh.tpt;
+        c.flags = sh.sort ? (cfg->flags | P2Z_FLAG_SORT_WINDOWS) : (cfg->flags & ~P2Z_FLAG_SORT_WINDOWS);
         r = p2z_run_device(ctx, &c, T, H, (const uint32_t *)M, O, st, nullptr);  // warm-up (graph capture)
         if (r != P2Z_OK) return r;
         TUNE_CUDA(ctx, cudaEventRecord(e0, st));
@@ -287,6 +292,7 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
         t.schedule = sh.sched;
         t.block_threads = sh.block;
         t.threads_per_track = sh.tpt;
+        t.flags = sh.sort ? P2Z_FLAG_SORT_WINDOWS : 0u;
         t.ms = ms / reps;
         t.updates_per_s = t.ms > 0 ? (double)s0.updates / (t.ms * 1e-3) : 0.0;
         if (n < max_entries) entries[n] = t;
@@ -296,7 +302,9 @@ p2z_status p2z_autotune(p2z_context *ctx, const p2z_config *cfg, const void *d_t
       c.schedule = P2Z_SCHED_AUTO;
       c.block_threads = 0;
       c.threads_per_track = 0;
-      r = record_tuned(ctx, &c, masked, local.block_threads, local.schedule, local.threads_per_track);
+      c.flags = cfg->flags;
+      r = record_tuned(ctx, &c, masked, local.block_threads, local.schedule, local.threads_per_track,
+                       (local.flags & P2Z_FLAG_SORT_WINDOWS) != 0);
       if (r != P2Z_OK) return r;
       if (top.ms < 0 || local.ms < top.ms) top = local;
     }

@@ -206,9 +206,13 @@ def test_autotune_contract(p2z, masked):
         torch.cuda.synchronize()
         best, rows = c.autotune(cfg, dt, dh, d_mask=dm, reps=2)
         # bsize x layout x (flat, persistent, per-event) x threads per track {1, 2} x block,
+        # masked: x window sorting {off, on} for flat and persistent,
         # + the staged schedule (one thread per track) at bsize 32 AOSOA
-        assert len(rows) == 4 * 2 * 3 * 2 * 4 + 4
+        per_bl = (2 * 2 + 1) * 2 * 4 if masked else 3 * 2 * 4
+        assert len(rows) == 4 * 2 * per_bl + 4
         assert {r["threads_per_track"] for r in rows} == {1, 2}
+        assert {r["sorted_windows"] for r in rows} == ({False, True} if masked else {False})
+        assert not any(r["sorted_windows"] for r in rows if r["schedule"] in ("per_event", "staged"))
         assert {r["threads_per_track"] for r in rows if r["schedule"] == "staged"} == {1}
         assert {r["bsize"] for r in rows} == {8, 16, 32, 64}
         assert {r["layout"] for r in rows} == {"aosoa", "soa"}
