@@ -641,7 +641,7 @@ class Context:
         _check(lib.p2z_unpack_tracks_device(self.h, C.byref(cfg), _ptr(d_perm), _ptr(d_trk_packed), _ptr(d_trk_out),
                                             stream), self.h)
 
-    def autotune(self, cfg: Config, d_trk_in, d_hits, d_mask=None, reps=3, max_entries=256):
+    def autotune(self, cfg: Config, d_trk_in, d_hits, d_mask=None, reps=3, max_entries=1024):
         """Measure every bsize x layout x schedule x block size (p2z_autotune).
         Returns (best, entries) as dicts, entries sorted by time."""
         rows = (TuneEntry * max_entries)()
