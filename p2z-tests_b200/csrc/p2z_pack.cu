@@ -11,7 +11,6 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 
-#include <algorithm>
 #include <cstdio>
 #include <vector>
 
@@ -70,15 +69,14 @@ __global__ void k_pack_keys(const uint32_t *__restrict__ mask, const int64_t *__
 // contiguous): word r of slot s is at (s / B) * bw + s % B + r * B.
 __device__ __forceinline__ int64_t slot_base(int64_t s, int B, int64_t bw) { return (s / B) * bw + s % B; }
 
-// Thread = slot s of the packed order, copying all `rows` words of a slot:
-// GATHER dst[s] = src[perm[s]] (packing), else dst[perm[s]] = src[s] (unpacking).
-template <bool GATHER>
-__global__ void k_permute(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
-                          const int64_t *__restrict__ perm, int64_t nslots, int B, int rows, int64_t bw) {
+// Thread = destination slot s, copying all `rows` words of a slot: dst[s] =
+// src[perm[s]] (packing with the permutation, unpacking with its inverse).
+// Consecutive threads write consecutive slots.
+__global__ void k_gather(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
+                         const int64_t *__restrict__ perm, int64_t nslots, int B, int rows, int64_t bw) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots) return;
-  const int64_t p = perm[s];
-  const int64_t from = slot_base(GATHER ? p : s, B, bw), to = slot_base(GATHER ? s : p, B, bw);
+  const int64_t from = slot_base(perm[s], B, bw), to = slot_base(s, B, bw);
 #pragma unroll 4
   for (int r = 0; r < rows; ++r) dst[to + (int64_t)r * B] = src[from + (int64_t)r * B];
 }
@@ -96,7 +94,7 @@ __global__ void k_gather_mask(const uint32_t *__restrict__ src, uint32_t *__rest
 }
 
 // Event tables of a config: per-event real tracks and first slots (nevts + 1).
-bool event_tables(const p2z_config *c, std::vector<int64_t> &counts, std::vector<int64_t> &beg) {
+void event_tables(const p2z_config *c, std::vector<int64_t> &counts, std::vector<int64_t> &beg) {
   const int64_t ne = c->nevts;
   counts.assign((size_t)ne, 0);
   beg.assign((size_t)ne + 1, 0);
@@ -104,7 +102,6 @@ bool event_tables(const p2z_config *c, std::vector<int64_t> &counts, std::vector
     counts[e] = c->event_ntrks ? c->event_ntrks[e] : c->ntrks;
     beg[e + 1] = beg[e] + (counts[e] + c->bsize - 1) / c->bsize * c->bsize;
   }
-  return true;
 }
 
 p2z_status check_config(p2z_context *ctx, const p2z_config *cfg, int64_t *nslots) {
@@ -167,9 +164,9 @@ p2z_status p2z_pack_by_hits_device(p2z_context *ctx, const p2z_config *cfg, cons
   PACK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, (const uint64_t *)keys, (uint64_t *)keys_sorted,
                                                  (const int64_t *)idx, d_perm, ns, 0, end_bit, st));
   const int B = cfg->bsize, nl = cfg->nlayer;
-  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_trk_in, (uint32_t *)d_trk_out, d_perm, ns, B, TRK_WORDS,
+  k_gather<<<gx, 256, 0, st>>>((const uint32_t *)d_trk_in, (uint32_t *)d_trk_out, d_perm, ns, B, TRK_WORDS,
                                       (int64_t)TRK_WORDS * B);
-  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_hits_in, (uint32_t *)d_hits_out, d_perm, ns, B,
+  k_gather<<<gx, 256, 0, st>>>((const uint32_t *)d_hits_in, (uint32_t *)d_hits_out, d_perm, ns, B,
                                       HIT_WORDS * nl, (int64_t)HIT_WORDS * nl * B);
   if (d_mask_in) k_gather_mask<<<gx, 256, 0, st>>>(d_mask_in, d_mask_out, d_perm, ns);
   k_invert<<<gx, 256, 0, st>>>(d_perm, d_perm + ns, ns);
@@ -194,7 +191,7 @@ p2z_status p2z_unpack_tracks_device(p2z_context *ctx, const p2z_config *cfg, con
   cudaStream_t st = stream ? (cudaStream_t)stream : context_stream(ctx);
   const unsigned gx = (unsigned)((ns + 255) / 256);
   // a gather through the inverse permutation (d_perm's second half): the writes are coalesced
-  k_permute<true><<<gx, 256, 0, st>>>((const uint32_t *)d_trk_packed, (uint32_t *)d_trk_out, d_perm + ns, ns,
+  k_gather<<<gx, 256, 0, st>>>((const uint32_t *)d_trk_packed, (uint32_t *)d_trk_out, d_perm + ns, ns,
                                       cfg->bsize, TRK_WORDS, (int64_t)TRK_WORDS * cfg->bsize);
   PACK_CUDA(ctx, cudaGetLastError());
   return P2Z_OK;
