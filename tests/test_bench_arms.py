@@ -54,3 +54,35 @@ def test_reference_arm_loads_no_product_library_and_shares_the_config(oracle):
     import importlib
     bench = importlib.import_module("bench")
     assert line["config"] == bench.workload_config(1000, 1)
+
+
+def _bench_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("p2z_bench_helpers", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_window_utilisation_and_tune_summary():
+    """The bench's lane-utilisation count for sorted windows and its summary of
+    an autotune sweep, on inputs whose answers are known."""
+    import torch
+    bench = _bench_module()
+    # 64 slots: window 1 holds 32 tracks of 20 hits and 32 of 4; sorted per 64-slot window the
+    # two warps take 20 and 4 steps (all lanes busy); per 32-slot window (no reordering across
+    # warps) each warp takes 20 steps for 16 x 20 + 16 x 4 hits
+    hits = [20, 4] * 32
+    mask = torch.tensor([(1 << h) - 1 for h in hits], dtype=torch.int64).to(torch.int32)
+    assert bench.window_util(mask, 64) == pytest.approx(1.0)
+    assert bench.window_util(mask, 32) == pytest.approx((16 * 20 + 16 * 4) / (32 * 20))
+    rows = [dict(bsize=b, layout=l, schedule=s, block_threads=32, threads_per_track=t, sorted_windows=w,
+                 ms=1.0 + 0.1 * b + (0.5 if l == "soa" else 0) + t + (0 if w else 0.05), updates_per_s=1.0)
+            for b in (8, 32) for l in ("aosoa", "soa") for s in ("flat", "persistent") for t in (1, 2)
+            for w in (False, True)]
+    best = min(rows, key=lambda r: r["ms"])
+    out = bench.tune_summary(best, rows, 1.5)
+    assert out["configurations"] == len(rows) and out["best"] is best
+    assert out["best_bsize32_aosoa"]["bsize"] == 32 and out["best_bsize32_aosoa"]["layout"] == "aosoa"
+    assert set(out["best_per_sorted_windows"]) == {"False", "True"}
+    assert out["best_per_threads_per_track"]["1"]["ms"] < out["best_per_threads_per_track"]["2"]["ms"]
