@@ -304,9 +304,12 @@ void worker_loop(p2z_server *s) {
     if (s->inflight.empty() && s->pending.empty() && s->admitted.empty()) {
       s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
     } else {
-      // poll the GPU without holding the lock for long
+      // poll the GPU without holding the lock for long: yield for a few
+      // microseconds (a sleep of that length lasts the OS timer slack, tens of
+      // microseconds, which every request's latency would carry)
       lk.unlock();
-      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(5);
+      while (std::chrono::steady_clock::now() < until) std::this_thread::yield();
       lk.lock();
     }
   }

@@ -18,17 +18,19 @@ def _events(p2z, counts, seed, nlayer=20, B=32, masks=True):
 
 
 def test_event_alone_equals_event_in_mix(p2z, ctx):
-    evs = _events(p2z, [3000, 50, 777, 20000, 1, 0, 4096, 1500], seed=40)
-    with p2z.Server(bsize=32, nlayer=20, budget_bytes=2 << 30) as srv:
+    # the 20000-track event first, with one group in flight: the others are submitted while its
+    # group (copies of ~17 MB, then the kernel) runs, so they are admitted together and mixed
+    evs = _events(p2z, [20000, 3000, 50, 777, 1, 0, 4096, 1500], seed=40)
+    with p2z.Server(bsize=32, nlayer=20, budget_bytes=2 << 30, max_inflight=1) as srv:
         # alone, one at a time
         alone = []
         for t, h, m, n, _ in evs:
             out = np.zeros_like(t)
             srv.wait(srv.submit(t, h, m, n, out))
             alone.append(out)
-        # all at once: admitted together, launched in mixed groups
-        ids = [srv.submit(t, h, m, n, o) for (t, h, m, n, o) in evs]
-        infos = [srv.wait(i) for i in ids]
+        # all at once (submitted back to back by the library's replay loop): while the first
+        # group runs the others are admitted together and launched in mixed groups
+        infos = srv.replay(evs, [0.0] * len(evs))
     assert max(inf.group_events for inf in infos) > 1
     for (t, h, m, n, o), a in zip(evs, alone):
         assert np.array_equal(o.view(np.uint32), a.view(np.uint32))
