@@ -142,9 +142,11 @@ typedef enum p2z_layout {
                                        the same.  On the uneven benchmark sample lane utilisation
                                        rises from 60% to 85% and the persistent pass is 13% faster;
                                        a warp's loads then reach 4 batches, so on even work (every
-                                       mask alike) it only costs.  Packing an event's tracks in order
-                                       of hit count when the arrays are built gains more (99%) and
-                                       costs nothing per pass */
+                                       mask alike) it only costs.  p2z_autotune measures both for
+                                       masked runs, and runs with schedule AUTO sort when that
+                                       measured faster.  Packing an event's tracks in order of hit
+                                       count (p2z_pack_by_hits_device, or when the arrays are built)
+                                       gains more (99%) */
 #define P2Z_FLAG_REFERENCE_ROUNDING 0x20u /* P2Z_UPDATE_V2 only: evaluate the reference's own FP32
                                        expressions, type promotions and operation order, every
                                        operation separately rounded, with correctly rounded
