@@ -97,3 +97,35 @@ def test_pair_refusals(p2z, ctx):
             ctx.run_device(cfg, t, h, torch.empty_like(t))
         assert e.value.status == p2z.UNSUPPORTED, kw
         assert "one thread per track" in str(e.value) or "threads_per_track" in str(e.value)
+
+
+@pytest.mark.parametrize("layout", ["b8", "b64", "soa"])
+def test_pair_and_sorted_windows_every_layout(p2z, ctx, layout):
+    """Two threads per track and sorted windows together and apart, flat and
+    persistent, on the bsizes and the layout the other tests use least:
+    every combination gives the one-thread, stored-order bits."""
+    counts = np.array([300, 0, 65, 1, 1000, 129], dtype=np.int64)
+    B = 32 if layout == "soa" else int(layout[1:])
+    cfg = p2z.make_config(bsize=B, nevts=len(counts), event_ntrks=counts, nlayer=20)
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    p2z.mask_layers(m, 20, min_hits=3, max_hits=20, drop_prob=0.2, seed=61)
+    if layout == "soa":
+        t, h = p2z.tracks_to_soa(t), p2z.hits_to_soa(h)
+        cfg.layout = p2z.LAYOUT_SOA
+    ref, _ = _run(p2z, ctx, cfg, t, h, m, schedule="flat", block_threads=64, threads_per_track=1, flags=0)
+    for sched in ("flat", "persistent"):
+        for tpt in (1, 2):
+            for flags in (0, p2z.FLAG_SORT_WINDOWS):
+                out, _ = _run(p2z, ctx, cfg, t, h, m, schedule=sched, block_threads=128, threads_per_track=tpt,
+                              flags=flags)
+                _same(out, ref)
+
+
+def test_pair_with_32_layers(p2z, ctx):
+    """Every mask bit, bit 31 included, with two threads per track."""
+    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=320, nlayer=32)
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    p2z.mask_layers(m, 32, min_hits=5, max_hits=32, drop_prob=0.1, seed=3)
+    ref, _ = _run(p2z, ctx, cfg, t, h, m, schedule="flat", block_threads=64, threads_per_track=1)
+    out, _ = _run(p2z, ctx, cfg, t, h, m, schedule="persistent", block_threads=64, threads_per_track=2)
+    _same(out, ref)
