@@ -86,3 +86,34 @@ def test_pack_without_mask_is_identity_and_refusals(p2z, ctx):
     with pytest.raises(p2z.P2zError) as e:
         ctx.pack_by_hits_device(cfg, dt, dh, pt, ph, perm)
     assert e.value.status == p2z.UNSUPPORTED
+
+
+@pytest.mark.parametrize("bsize", [16, 64])
+def test_pack_every_event_size(p2z, ctx, bsize):
+    """Events of every size the packing's gathers distinguish: from one batch
+    to above 32768 slots (too large for shared memory, read directly), empty
+    events among them; the order, the packed words and the round trip."""
+    import torch
+    counts = np.array([40000, 7, 20000, 0, 9000, 5000, 2100, 1500, 600, 300, 100, 1], dtype=np.int64)
+    cfg = p2z.make_config(bsize=bsize, nevts=len(counts), event_ntrks=counts, nlayer=12, schedule="flat")
+    t, h, m = p2z.generate_physics(cfg, with_mask=True)
+    p2z.mask_layers(m, 12, min_hits=3, max_hits=12, drop_prob=0.2, seed=43)
+    nb = p2z.num_batches(cfg)
+    dt, dh, dm = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda(), torch.from_numpy(m.view(np.int32)).cuda()
+    pt, ph, pm = torch.empty_like(dt), torch.empty_like(dh), torch.empty_like(dm)
+    perm = torch.empty(2 * nb * bsize, dtype=torch.int64, device="cuda")
+    ctx.pack_by_hits_device(cfg, dt, dh, pt, ph, perm, d_mask_in=dm, d_mask_out=pm)
+    torch.cuda.synchronize()
+    got = perm.cpu().numpy()[:nb * bsize]
+    assert np.array_equal(got, _expected_perm(counts, m, bsize, 12))
+    T, H = p2z.tracks_to_soa(t), p2z.hits_to_soa(h)
+    assert np.array_equal(p2z.tracks_to_soa(pt.cpu().numpy()).view(np.uint32), T[:, got].view(np.uint32))
+    assert np.array_equal(p2z.hits_to_soa(ph.cpu().numpy()).view(np.uint32), H[:, :, got].view(np.uint32))
+    assert np.array_equal(pm.cpu().numpy().view(np.uint32), m[got])
+    ref = torch.empty_like(dt)
+    ctx.run_device(cfg, dt, dh, ref, d_mask=dm)
+    po, back = torch.empty_like(dt), torch.full_like(dt, float("nan"))
+    ctx.run_device(cfg, pt, ph, po, d_mask=pm)
+    ctx.unpack_tracks_device(cfg, perm, po, back)
+    torch.cuda.synchronize()
+    assert np.array_equal(back.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
