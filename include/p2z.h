@@ -241,10 +241,13 @@ size_t p2z_sizeof_mphit(int bsize);   /* 9*bsize*4 */
  * copied asynchronously; pageable ones go through a staging path.  The work is
  * split into up to 16 chunks whose copies and passes alternate between two
  * streams.  With page-locked buffers (all of trk_in, hits, trk_out and
- * hit_mask when given) the whole pipeline is recorded as a CUDA graph on the
- * first call and replayed by later calls with the same config, host buffers
- * and internal device buffers, so that a call costs one graph launch; a call
- * that differs in any of them records again.  P2Z_FLAG_NO_GRAPH enqueues
+ * hit_mask when given) and a pipeline of 4 or more chunk passes (256 or more
+ * batches; chunks x niter) or per-event launches (events x niter), the whole
+ * pipeline is recorded as a CUDA graph on the first call and replayed by later
+ * calls with the same config, host buffers and internal device buffers, so
+ * that a call costs one graph launch; a call that differs in any of them
+ * records again.  Shorter pipelines are enqueued directly, which lets their
+ * first copy start while the rest is enqueued.  P2Z_FLAG_NO_GRAPH enqueues
  * every copy and kernel directly.  Synchronous: returns when trk_out holds
  * the results. */
 p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, const void *hits,

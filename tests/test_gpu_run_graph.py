@@ -1,6 +1,7 @@
 """p2z_run with page-locked host buffers records its copy/kernel pipeline as a
 CUDA graph on the first call and replays it while the config and buffers stay
-the same.  Checked against the same calls with P2Z_FLAG_NO_GRAPH (every copy
+the same (pipelines of 4 or more chunk passes or per-event launches: every
+case below is that long except the short page-locked call, enqueued directly).  Checked against the same calls with P2Z_FLAG_NO_GRAPH (every copy
 and kernel enqueued directly) and against p2z_run_device on the same inputs,
 bit for bit: uniform and uneven runs (internal padding mask and a caller's hit
 mask), the per-event schedule with and without its 10 streams, sorted windows,
@@ -38,7 +39,7 @@ CASES = ["uniform", "uneven_internal_mask", "uneven_user_mask", "per_event", "pe
 
 @pytest.mark.parametrize("case", CASES)
 def test_run_graph_matches_direct_and_device(p2z, ctx, case):
-    counts = np.array([50, 1, 0, 777, 3000, 31, 64, 4000, 2], dtype=np.int64)
+    counts = np.array([50, 1, 0, 777, 3000, 31, 64, 4000, 2, 2100], dtype=np.int64)  # 317 batches: 4 chunks
     if case in ("uniform", "soa", "two_threads_per_track"):
         cfg = p2z.make_config(bsize=32, nevts=3, ntrks=4096, nlayer=20)
         t, h = p2z.generate_physics(cfg)
@@ -104,10 +105,20 @@ def test_run_graph_matches_direct_and_device(p2z, ctx, case):
             a.free()
 
 
-def test_run_graph_pageable_and_inplace(p2z, ctx):
-    """Pageable buffers take the direct path; in-place runs (trk_out ==
-    trk_in, page-locked) replay correctly."""
-    cfg = p2z.make_config(bsize=32, nevts=2, ntrks=2048, nlayer=20)
+def test_run_graph_pageable_short_and_inplace(p2z, ctx):
+    """Pageable buffers and short pipelines take the direct path; in-place runs
+    (trk_out == trk_in, page-locked) replay correctly."""
+    short = p2z.make_config(bsize=32, nevts=1, ntrks=1024, nlayer=20)  # 32 batches: one chunk
+    t, h = p2z.generate_physics(short)
+    ref = _device_ref(p2z, ctx, short, t, h, None)
+    pt, ph, po = _pinned(p2z, t), _pinned(p2z, h), p2z.PinnedArray(t.shape, t.dtype)
+    for _ in range(2):
+        po.array[...] = np.nan
+        ctx.run(short, pt.array, ph.array, po.array)
+        _same(po.array, ref)
+    for a in (pt, ph, po):
+        a.free()
+    cfg = p2z.make_config(bsize=32, nevts=4, ntrks=2048, nlayer=20)  # 256 batches: 4 chunks
     t, h = p2z.generate_physics(cfg)
     ref = _device_ref(p2z, ctx, cfg, t, h, None)
     out = np.full_like(t, np.nan)
