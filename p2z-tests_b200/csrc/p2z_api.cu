@@ -155,7 +155,7 @@ struct Plan {
   bool uneven = false;
   bool soa = false;          // P2Z_LAYOUT_SOA
   std::vector<int64_t> ev_slot_begin;  // nevts + 1 entries
-  std::vector<uint8_t> batch_valid;    // uneven: real lanes per batch
+  const int64_t *event_ntrks = nullptr;  // uneven: the caller's tracks per event
 };
 
 p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
@@ -203,14 +203,10 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
       const int64_t n = cfg->event_ntrks[e];
       if (n < 0) return fail(ctx, P2Z_BAD_ARG, "event_ntrks[%lld] = %lld < 0", (long long)e, (long long)n);
       pl.ev_slot_begin[e] = nb * pl.B;
-      const int64_t nbe = (n + pl.B - 1) / pl.B;
-      for (int64_t i = 0; i < nbe; ++i) {
-        const int64_t left = n - i * pl.B;
-        pl.batch_valid.push_back((uint8_t)(left >= pl.B ? pl.B : left));
-      }
-      nb += nbe;
+      nb += (n + pl.B - 1) / pl.B;
     }
     pl.nbatches = nb;
+    pl.event_ntrks = cfg->event_ntrks;
     pl.ev_slot_begin[cfg->nevts] = nb * pl.B;
   } else {
     if (cfg->ntrks < 0 || cfg->ntrks % cfg->bsize)
@@ -488,9 +484,23 @@ int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool mas
   return masked ? P2Z_SCHED_PERSISTENT : P2Z_SCHED_FLAT;
 }
 
+// Real lanes per batch of uneven events (built only where the padding mask
+// needs it: one byte per batch).
+std::vector<uint8_t> batch_valid(const Plan &pl) {
+  std::vector<uint8_t> v;
+  v.reserve((size_t)pl.nbatches);
+  const int64_t nev = (int64_t)pl.ev_slot_begin.size() - 1;
+  for (int64_t e = 0; e < nev; ++e) {
+    const int64_t n = pl.event_ntrks[e];
+    for (int64_t left = n; left > 0; left -= pl.B) v.push_back((uint8_t)(left >= pl.B ? pl.B : left));
+  }
+  return v;
+}
+
 // Builds the padding mask of uneven events into ctx->valid / ctx->mask.
 p2z_status internal_mask(p2z_context *ctx, const Plan &pl, cudaStream_t st, const uint32_t **out) {
-  p2z_status r = ensure(ctx, ctx->valid, pl.batch_valid.size());
+  const std::vector<uint8_t> valid = batch_valid(pl);
+  p2z_status r = ensure(ctx, ctx->valid, valid.size());
   if (r != P2Z_OK) return r;
   r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots);
   if (r != P2Z_OK) return r;
@@ -498,7 +508,8 @@ p2z_status internal_mask(p2z_context *ctx, const Plan &pl, cudaStream_t st, cons
     *out = (const uint32_t *)ctx->mask.p;
     return P2Z_OK;
   }
-  P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->valid.p, pl.batch_valid.data(), pl.batch_valid.size(), cudaMemcpyHostToDevice, st));
+  // (pageable source: the copy is staged before the call returns)
+  P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->valid.p, valid.data(), valid.size(), cudaMemcpyHostToDevice, st));
   k_fill_mask<<<(unsigned)((pl.nslots + 255) / 256), 256, 0, st>>>((uint32_t *)ctx->mask.p, (const uint8_t *)ctx->valid.p,
                                                                    pl.nslots, pl.B, all_layers(pl.nlayer));
   P2Z_CUDA(ctx, cudaGetLastError());
