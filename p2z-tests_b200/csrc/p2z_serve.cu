@@ -100,6 +100,8 @@ struct p2z_server {
   unsigned long long *d_counters = nullptr;  // one persistent work counter per group slot
   unsigned int *d_status = nullptr;
   cudaStream_t copy = nullptr, compute = nullptr;
+  cudaEvent_t copied = nullptr;  // a group's copies issued (re-recorded for every group)
+  int occupancy = 0;             // resident CTAs per SM of the server's kernel (fixed per server)
   int max_inflight = 2;
 
   // ring
@@ -190,11 +192,8 @@ void launch_group(p2z_server *s) {
   std::vector<int64_t> ids(s->admitted.begin(), s->admitted.end());
   s->admitted.clear();
   // the group's copies were issued on the copy stream before this point
-  cudaEvent_t copied;
-  cudaEventCreateWithFlags(&copied, cudaEventDisableTiming);
-  cudaEventRecord(copied, s->copy);
-  cudaStreamWaitEvent(s->compute, copied, 0);
-  cudaEventDestroy(copied);
+  cudaEventRecord(s->copied, s->copy);
+  cudaStreamWaitEvent(s->compute, s->copied, 0);
   // contiguous runs of ring batches (a run breaks where the ring wraps)
   LaunchSpec spec;
   std::memset(&spec, 0, sizeof spec);
@@ -213,7 +212,8 @@ void launch_group(p2z_server *s) {
   spec.masked = true;
   spec.kind = KIND_PERSISTENT;
   spec.block = s->cfg.block_threads ? s->cfg.block_threads : 128;
-  const int occ = std::max(1, kernel_occupancy(spec));
+  if (s->occupancy == 0) s->occupancy = std::max(1, kernel_occupancy(spec));  // same kernel and block every group
+  const int occ = s->occupancy;
   const double t = now_s(s->t0);
   size_t i = 0;
   while (i < ids.size()) {
@@ -364,6 +364,7 @@ p2z_status p2z_server_create(int device, const p2z_server_config *cfg, p2z_serve
   if ((e = cudaMalloc(&s->d_status, sizeof(unsigned int))) != cudaSuccess) return bail(P2Z_OOM);
   if ((e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking)) != cudaSuccess) return bail(P2Z_CUDA_ERROR);
   if ((e = cudaStreamCreateWithFlags(&s->compute, cudaStreamNonBlocking)) != cudaSuccess) return bail(P2Z_CUDA_ERROR);
+  if ((e = cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming)) != cudaSuccess) return bail(P2Z_CUDA_ERROR);
   cudaMemset(s->d_status, 0, sizeof(unsigned int));
   s->worker = std::thread(worker_loop, s);
   *out = s;
@@ -386,6 +387,7 @@ p2z_status p2z_server_destroy(p2z_server *s) {
   for (auto &kv : s->reqs)
     if (kv.second.done_ev) cudaEventDestroy(kv.second.done_ev);
   for (cudaEvent_t ev : s->free_events) cudaEventDestroy(ev);
+  if (s->copied) cudaEventDestroy(s->copied);
   for (void *p : {(void *)s->d_trk, (void *)s->d_out, (void *)s->d_hit, (void *)s->d_mask, (void *)s->d_counters,
                   (void *)s->d_status})
     if (p) cudaFree(p);
