@@ -43,6 +43,31 @@
 #ifndef P2Z_H
 #define P2Z_H
 
+/* The reference's sources define their sizes as macros (bsize, nevts, ntrks,
+ * nlayer, nb, NITER, nthreads, smear, N: src/propagate-toz-test_OMP.cpp:18-41,
+ * :295) before any code.  They are set aside while this header compiles and
+ * restored at its end, so it can be included before or after them.  In code
+ * that sees those macros, fill a p2z_config with p2z_config_init: a member
+ * access such as cfg.bsize would expand the macro. */
+#pragma push_macro("bsize")
+#undef bsize
+#pragma push_macro("nevts")
+#undef nevts
+#pragma push_macro("ntrks")
+#undef ntrks
+#pragma push_macro("nlayer")
+#undef nlayer
+#pragma push_macro("nb")
+#undef nb
+#pragma push_macro("NITER")
+#undef NITER
+#pragma push_macro("nthreads")
+#undef nthreads
+#pragma push_macro("smear")
+#undef smear
+#pragma push_macro("N")
+#undef N
+
 #include <stddef.h>
 #include <stdint.h>
 
@@ -187,6 +212,16 @@ typedef struct p2z_config {
                             per track in every GPU version, src/propagate-toz-test_CUDA_v4.cu:
                             761-775) */
 } p2z_config;
+
+/* Fills *cfg for the uniform form: abi_version, the sizes given, one pass,
+ * P2Z_UPDATE_V2, and every other field 0 (P2Z_SCHED_AUTO, block size and
+ * threads per track from the autotuner or their defaults, no flags, AOSOA,
+ * P2Z_KFACT_DEFAULT, no event_ntrks).  Callers whose code defines the
+ * reference's size macros pass them here
+ * (p2z_config_init(&cfg, bsize, nevts, ntrks, nlayer)) instead of writing
+ * cfg.bsize = bsize, which the macros would expand.  Checks nothing but cfg:
+ * the run entry points validate the config. */
+p2z_status p2z_config_init(p2z_config *cfg, int32_t bsize, int64_t nevts, int64_t ntrks, int32_t nlayer);
 
 /* Filled by the run entry points (optional out-parameter). */
 typedef struct p2z_stats {
@@ -655,5 +690,15 @@ p2z_status p2z_copy(p2z_context *ctx, void *dst, const void *src, size_t bytes);
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
+
+#pragma pop_macro("N")
+#pragma pop_macro("smear")
+#pragma pop_macro("nthreads")
+#pragma pop_macro("NITER")
+#pragma pop_macro("nb")
+#pragma pop_macro("nlayer")
+#pragma pop_macro("ntrks")
+#pragma pop_macro("nevts")
+#pragma pop_macro("bsize")
 
 #endif /* P2Z_H */

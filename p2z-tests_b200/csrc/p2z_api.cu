@@ -600,6 +600,19 @@ p2z_status record_tuned(p2z_context *ctx, const p2z_config *cfg, bool masked, in
 
 extern "C" {
 
+p2z_status p2z_config_init(p2z_config *cfg, int32_t bsize, int64_t nevts, int64_t ntrks, int32_t nlayer) {
+  if (!cfg) return fail(nullptr, P2Z_BAD_ARG, "config is NULL");
+  std::memset(cfg, 0, sizeof *cfg);
+  cfg->abi_version = P2Z_ABI_VERSION;
+  cfg->bsize = bsize;
+  cfg->nevts = nevts;
+  cfg->ntrks = ntrks;
+  cfg->nlayer = nlayer;
+  cfg->niter = 1;
+  cfg->update = P2Z_UPDATE_V2;
+  return P2Z_OK;
+}
+
 const char *p2z_status_string(p2z_status s) {
   switch (s) {
     case P2Z_OK: return "ok";

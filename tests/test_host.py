@@ -20,6 +20,29 @@ def test_library_exports_every_declared_symbol(p2z):
     assert not missing, missing
 
 
+@pytest.mark.parametrize("lang", ["c", "c++"])
+@pytest.mark.parametrize("bsize", [8, 32])
+def test_c_abi_after_the_reference_macros(tmp_path, lang, bsize):
+    """p2z.h included after the reference's size macros, as a maintainer adds
+    it to the OpenMP source; the config filled by p2z_config_init from those
+    macros; the macros intact after the header.  Compiled as C and as C++."""
+    exe = tmp_path / "c_abi_macros"
+    cc = ["gcc", "-std=c11"] if lang == "c" else ["g++", "-std=c++17", "-x", "c++"]
+    pkg = ROOT / "p2z-tests_b200"
+    cmd = [*cc, "-O2", "-Wall", "-Werror", f"-I{ROOT / 'include'}", f"-Dbsize={bsize}",
+           str(ROOT / "tests" / "cpp" / "c_abi_macros.c"), "-x", "none", "-o", str(exe), f"-L{pkg}", "-lp2z",
+           f"-Wl,-rpath,{pkg}"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    lines = r.stdout.splitlines()
+    assert lines[0] == "abi_version 2"
+    assert lines[1] == f"sizes {bsize} 100 9600 20"
+    assert lines[2] == "niter 5 update 0 schedule 0 block 0 flags 0 layout 0 tpt 0 kfact 0 event_ntrks 0"
+    assert lines[3] == f"batches {100 * 9600 // bsize}"
+
+
 def test_version_and_sizes(p2z):
     assert p2z.lib.p2z_version(None, 0) == p2z.ABI_VERSION
     assert "sm_100a" in p2z.version()
