@@ -145,7 +145,14 @@ typedef enum p2z_layout {
 } p2z_layout;
 
 /* Flags */
-#define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan inputs for NaN/Inf first -> P2Z_NONFINITE_INPUT */
+#define P2Z_FLAG_CHECK_INPUTS 0x1u  /* scan the input words the pass reads for NaN/Inf ->
+                                       P2Z_NONFINITE_INPUT: the 27 floating-point track words of
+                                       every slot with a present layer and, on each present layer,
+                                       the hit words the update kind reads (6 for the 2-D updates,
+                                       9 for the 3-D ones); padding slots and absent layers are not
+                                       read and not scanned.  p2z_run_device: before the pass,
+                                       synchronously, and the pass does not run; p2z_run: each
+                                       chunk after its copy, the pass still runs */
 #define P2Z_FLAG_STRICT       0x2u  /* return P2Z_SINGULAR if any det <= 0 was met */
 #define P2Z_FLAG_NO_GRAPH     0x4u  /* PERSISTENT, and p2z_run with page-locked buffers: enqueue
                                        directly instead of replaying a recorded graph */
@@ -296,7 +303,15 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
  * which case it synchronises to fill the timings.  The PERSISTENT schedule's
  * graph is recorded on the context's stream and replayed on `stream`; while
  * `stream` is itself being captured, the kernels are launched into it directly.
- * d_trk_out must not alias d_trk_in.  Replaces GPUsequence/GPUsequenceR
+ * d_trk_out must not alias d_trk_in.  Calls on one context whose work
+ * overlaps on the GPU (different streams, as the reference's GPU build issues
+ * its chunks) share the context's device scratch: with the FLAT schedule
+ * (the rule for runs without masks) and the default flags they share only the
+ * status word, whose bits the kernels only set, and may overlap; with the
+ * PERSISTENT or STAGED schedule (work counter), P2Z_FLAG_SORT_WINDOWS (window
+ * permutation), uneven events given without a mask (padding mask), stats or
+ * P2Z_FLAG_CHECK_INPUTS (status reset) they must not: order those streams, or
+ * use one context per stream.  Replaces GPUsequence/GPUsequenceR
  * (src/propagate-toz-test_CUDA_v4.cu:746-828). */
 p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d_trk_in, const void *d_hits,
                           const uint32_t *d_hit_mask, void *d_trk_out, void *stream, p2z_stats *stats);

@@ -484,6 +484,21 @@ int resolve_schedule(p2z_context *ctx, Plan &pl, const p2z_config *cfg, bool mas
   return masked ? P2Z_SCHED_PERSISTENT : P2Z_SCHED_FLAT;
 }
 
+// Hit words an update kind reads per present layer: the 2-D updates the first
+// 6 (x, y, z, V00, V10, V11), the 3-D ones all 9.
+int hit_words_read(int upd) { return (upd == UPDK_3X3_F64 || upd == UPDK_3X3_COMP) ? 9 : 6; }
+
+// P2Z_FLAG_CHECK_INPUTS: the scan of slots [s0, s1) on st (status bit 2).
+p2z_status enqueue_check(p2z_context *ctx, const Plan &pl, const RunArgs &base, int64_t s0, int64_t s1,
+                         cudaStream_t st) {
+  RunArgs a = base;
+  a.slot_begin = s0;
+  a.slot_end = s1;
+  a.ws = pl.nslots;
+  P2Z_CUDA(ctx, launch_check_inputs(a, pl.soa ? 0 : pl.B, hit_words_read(pl.upd), st));
+  return P2Z_OK;
+}
+
 // Real lanes per batch of uneven events (built only where the padding mask
 // needs it: one byte per batch).
 std::vector<uint8_t> batch_valid(const Plan &pl) {
@@ -748,6 +763,16 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
   base.status = ctx->d_status;
   const int schedule = resolve_schedule(ctx, pl, cfg, mask != nullptr);
   int launches = 0;
+  if ((pl.flags & P2Z_FLAG_CHECK_INPUTS) && pl.nslots > 0) {
+    // synchronous: the pass runs only on finite inputs
+    P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
+    r = enqueue_check(ctx, pl, base, 0, pl.nslots, st);
+    if (r != P2Z_OK) return r;
+    P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    P2Z_CUDA(ctx, cudaStreamSynchronize(st));
+    if (*(volatile unsigned int *)ctx->h_status & 4u)
+      return fail(ctx, P2Z_NONFINITE_INPUT, "a track or hit word the pass reads is NaN or Inf");
+  }
   if (stats) {
     P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
     P2Z_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
@@ -827,6 +852,8 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
   const int64_t cb = nchunk ? (pl.nbatches + nchunk - 1) / nchunk : 0;
   int launches = 0;
   int64_t h2d = 0, d2h = 0;
+  // P2Z_FLAG_CHECK_INPUTS: each chunk is scanned after its copies, before its pass
+  const bool check = (pl.flags & P2Z_FLAG_CHECK_INPUTS) != 0;
   // The work of one call on the two copy streams: the status reset, then per
   // chunk the host->device copies, the pass and the device->host copy,
   // alternating between s0 and s1 (s1 forks from and joins back into s0).
@@ -865,6 +892,10 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
           P2Z_CUDA(ctx, cudaMemcpyAsync((char *)ctx->mask.p + b0 * pl.B * 4, (const char *)hit_mask + b0 * pl.B * 4,
                                         nbc * pl.B * 4, cudaMemcpyHostToDevice, st));
           h2d += nbc * pl.B * 4;
+        }
+        if (check) {
+          r = enqueue_check(ctx, pl, base, b0 * pl.B, b1 * pl.B, st);
+          if (r != P2Z_OK) return r;
         }
         if (!per_event) {
           r = enqueue_pass(ctx, pl, base, b0 * pl.B, b1 * pl.B,
@@ -975,6 +1006,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
     r = count_updates(ctx, pl, d_mask, s0, &stats->updates);
     if (r != P2Z_OK) return r;
   }
+  if (status & 4u) return fail(ctx, P2Z_NONFINITE_INPUT, "a track or hit word the pass read is NaN or Inf");
   if ((pl.flags & P2Z_FLAG_STRICT) && (status & 1u))
     return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
   return P2Z_OK;

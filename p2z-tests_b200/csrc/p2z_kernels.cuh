@@ -677,6 +677,11 @@ struct LaunchSpec {
   int tpt;       // threads per track: 1, or 2 (UPDK_V2, flat and persistent kinds)
 };
 
+// P2Z_FLAG_CHECK_INPUTS (p2z_check.cu): sets status bit 2 when a word the
+// pass over slots [a.slot_begin, a.slot_end) reads is NaN or Inf; B = 0: SoA
+// (word stride a.ws); nh hit words per present layer.
+cudaError_t launch_check_inputs(const RunArgs &a, int B, int nh, cudaStream_t st);
+
 // Per-update-kind dispatchers (one translation unit each).
 cudaError_t launch_v2(const LaunchSpec &s, cudaStream_t st);
 cudaError_t launch_v2_comp(const LaunchSpec &s, cudaStream_t st);
