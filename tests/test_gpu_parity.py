@@ -182,6 +182,32 @@ def test_reference_rounding_bit_exact_physics(p2z, oracle, ctx, physics):
     assert nd == 0
 
 
+@pytest.mark.parametrize("kfact,precise", [(100.0 / (-0.299792458 * 3.8), True),
+                                           (100.0 / (-0.299792458 * 2.0), False)])
+def test_custom_field_constant(p2z, oracle, ctx, physics, kfact, precise):
+    """p2z_config.kfact other than the OMP family's (a 3.8 T and a 2 T field):
+    the reference-rounding form bit for bit against the FP32 oracle given the
+    same constant; at 3.8 T, where the physics sample's hits (made at 3.8112 T)
+    stay near the propagated tracks, the precise form within the parity
+    tolerance of the FP64 oracle given the constant; kfact = 0 the same bits as
+    the default constant."""
+    trk, hit = physics
+    t, h = trk[:60].copy(), hit[:60].copy()
+    kf = float(np.float32(kfact))
+
+    def go(flags, k):
+        cfg = p2z.make_config(bsize=32, nevts=2, ntrks=960, nlayer=20, flags=flags, kfact=k)
+        out = np.empty_like(t)
+        ctx.run(cfg, t, h, out)
+        return out
+    assert _bitdiff(go(p2z.FLAG_REFERENCE_ROUNDING, kf), oracle.run_f32(t, h, kfact=kf, cr_trig=True)) == 0
+    if precise:
+        got = p2z.tracks_to_aos(go(0, kf))["par"]
+        ref = oracle.run_f64(t, h, kfact=kf)[:, :6]
+        assert par_rel(got, ref).max() <= PREC_PAR
+    assert _bitdiff(go(0, 0.0), go(0, oracle.kfact_default())) == 0
+
+
 def test_reference_rounding_within_reference_build_spread(p2z, oracle, ctx, physics):
     """Against the reference as its Makefile builds it (FMA contraction, glibc
     sinf/cosf): within the spread the reference itself shows between its
