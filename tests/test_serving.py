@@ -102,3 +102,32 @@ def test_poll_wait_timeout_and_release(p2z):
         assert np.isfinite(o.array[:, :6, :]).all()
     finally:
         t.free(); h.free(); o.free()
+
+
+SERVER_CONFIGS = [
+    ("v2", 0, 0.0), ("v2", "reference_rounding", 0.0), ("v2", "accurate_trig", 0.0), ("v2", "full_hits", 0.0),
+    ("v2_comp", 0, 0.0), ("3x3_f64", 0, 0.0), ("3x3_comp", 0, 0.0), ("f64", 0, 0.0),
+    ("v2", 0, 100.0 / (-0.299792458 * 3.8)),
+]
+
+
+@pytest.mark.parametrize("update,flag,kfact", SERVER_CONFIGS)
+def test_server_kinds_and_flags_match_p2z_run(p2z, ctx, update, flag, kfact):
+    """Every update kind and flag the server takes (the 3-D kinds copy all 9
+    hit words, the 2-D ones 6 unless P2Z_FLAG_FULL_HITS) and a field constant
+    of its own: each event's result, submitted in a mix, equals a p2z_run of
+    the same event with the same kind, flags and constant, bit for bit."""
+    flags = {0: 0, "reference_rounding": p2z.FLAG_REFERENCE_ROUNDING, "accurate_trig": p2z.FLAG_ACCURATE_TRIG,
+             "full_hits": p2z.FLAG_FULL_HITS}[flag]
+    kf = float(np.float32(kfact))
+    evs = _events(p2z, [2000, 31, 777, 0, 96], seed=300)
+    with p2z.Server(bsize=32, nlayer=20, update=update, flags=flags, kfact=kf, budget_bytes=1 << 30,
+                    max_inflight=2) as srv:
+        infos = srv.replay(evs, [0.0] * len(evs))
+    assert all(i.status == p2z.OK for i in infos)
+    for t, h, m, n, o in evs:
+        cfg = p2z.make_config(bsize=32, nevts=1, event_ntrks=[n], nlayer=20, update=update, flags=flags,
+                              kfact=kf, schedule="persistent")
+        ref = np.empty_like(t)
+        ctx.run(cfg, t, h, ref, hit_mask=m)
+        assert np.array_equal(ref.view(np.uint32), o.view(np.uint32)), (update, flag, n)
