@@ -299,8 +299,10 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
  * NULL = the context's stream, cudaStreamLegacy = the legacy default stream).
  * The context's stream is not ordered with any other: a caller whose buffers
  * come from work on another stream passes that stream, or synchronises it
- * first.  Returns after enqueueing (asynchronous) unless stats != NULL, in
- * which case it synchronises to fill the timings.  The PERSISTENT schedule's
+ * first.  Returns after enqueueing (asynchronous) unless stats != NULL (it
+ * then synchronises to fill the timings), P2Z_FLAG_STRICT is set (it
+ * synchronises to read the status: P2Z_SINGULAR, or P2Z_TIMEOUT from a staged
+ * wait) or P2Z_FLAG_CHECK_INPUTS is set (the scan before the pass).  The PERSISTENT schedule's
  * graph is recorded on the context's stream and replayed on `stream`; while
  * `stream` is itself being captured, the kernels are launched into it directly.
  * d_trk_out must not alias d_trk_in.  Calls on one context whose work

@@ -773,10 +773,11 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
     if (*(volatile unsigned int *)ctx->h_status & 4u)
       return fail(ctx, P2Z_NONFINITE_INPUT, "a track or hit word the pass reads is NaN or Inf");
   }
-  if (stats) {
-    P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
-    P2Z_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-  }
+  // the status word is read back for stats and, without them, for P2Z_FLAG_STRICT (the call then
+  // synchronises)
+  const bool strict_only = !stats && (pl.flags & P2Z_FLAG_STRICT) && pl.nslots > 0;
+  if (stats || strict_only) P2Z_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), st));
+  if (stats) P2Z_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
   for (int it = 0; it < pl.niter; ++it) {
     r = enqueue_pass(ctx, pl, base, 0, pl.nslots, schedule, st, ctx->d_queue, &launches);
     if (r != P2Z_OK) return r;
@@ -799,6 +800,12 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
     if (status & 2u) return fail(ctx, P2Z_TIMEOUT, "a staged kernel's wait for a bulk copy ran out");
     if ((pl.flags & P2Z_FLAG_STRICT) && stats->singular)
       return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
+  } else if (strict_only) {
+    P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    P2Z_CUDA(ctx, cudaStreamSynchronize(st));
+    const unsigned int status = *(volatile unsigned int *)ctx->h_status;
+    if (status & 2u) return fail(ctx, P2Z_TIMEOUT, "a staged kernel's wait for a bulk copy ran out");
+    if (status & 1u) return fail(ctx, P2Z_SINGULAR, "a residual covariance with det <= 0 was met");
   } else {
     P2Z_CUDA(ctx, cudaGetLastError());
   }

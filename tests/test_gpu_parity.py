@@ -412,10 +412,22 @@ def test_error_paths(p2z, ctx, physics):
     with pytest.raises(p2z.P2zError) as e:
         ctx.run(cfg, t, h, out)
     assert e.value.status == p2z.SINGULAR
+    # the same through p2z_run_device, with and without stats (strict mode synchronises to read the status)
+    import torch
+    dt, dh, do = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda(), torch.empty(t.shape, device="cuda")
+    for with_stats in (True, False):
+        with pytest.raises(p2z.P2zError) as e:
+            ctx.run_device(cfg, dt, dh, do, stats=with_stats)
+        assert e.value.status == p2z.SINGULAR, with_stats
+    cfg.flags = p2z.FLAG_STRICT
+    assert ctx.run_device(cfg, torch.from_numpy(trk[:1].copy()).cuda(), torch.from_numpy(hit[:1].copy()).cuda(), do,
+                          stats=False) is None  # finite, well-conditioned inputs: no error
     # without strict mode the run completes (NaNs propagate as in the reference)
     cfg.flags = 0
     st = ctx.run(cfg, t, h, out)
     assert st.singular == 1
+    ctx.run_device(cfg, dt, dh, do, stats=False)
+    torch.cuda.synchronize()
 
 
 def test_nonfinite_inputs_propagate_like_reference(p2z, oracle, ctx, physics):
