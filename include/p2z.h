@@ -320,9 +320,13 @@ p2z_status p2z_run_device(p2z_context *ctx, const p2z_config *cfg, const void *d
 
 /* One layer step on device buffers, in place on d_trk (nbatches MPTRK of width
  * bsize): what = 1 propagateToZ (src/propagate-toz-test_OMP.cpp:623-682),
- * 2 the measurement update selected by `update` (KalmanUpdate_v2, :503-620, for
- * P2Z_UPDATE_V2), 3 both.  The hits used are those of `layer` in the standard
- * hit array of nlayer layers.  Synchronous. */
+ * 2 KalmanUpdate_v2 (:503-620), 3 both.  `update` must be P2Z_UPDATE_V2 (any
+ * other kind returns P2Z_UNSUPPORTED: the step form exists for the
+ * reference's own layer loop).  The reference's FP32 expressions with every
+ * operation rounded separately (the P2Z_FLAG_REFERENCE_ROUNDING arithmetic),
+ * the full 21-element covariance (its z row may be non-zero); kfact 0 ->
+ * P2Z_KFACT_DEFAULT.  The hits used are those of `layer` in the standard hit
+ * array of nlayer layers.  Runs on the context's stream; synchronous. */
 p2z_status p2z_step_device(p2z_context *ctx, int bsize, int64_t nbatches, void *d_trk, const void *d_hits,
                            int nlayer, int layer, int what, int update, float kfact);
 
