@@ -141,6 +141,10 @@ class ClockSampler:
             self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(self._handle, nv.NVML_CLOCK_SM))
             self._thread = threading.Thread(target=self._poll, daemon=True)
             self._thread.start()
+            # return once the thread is sampling, so that the timed region that follows is covered
+            t_end = time.perf_counter() + 1.0
+            while len(self.samples) < 3 and self._thread.is_alive() and time.perf_counter() < t_end:
+                time.sleep(0.001)
             return
         except Exception:
             self._nvml = None
@@ -188,13 +192,18 @@ class ClockSampler:
                 except (ValueError, IndexError):
                     continue
         sel = [x for x in self.samples if x[0] is None or t0 is None or t0 <= x[0] <= t1]
+        window = "timed region"
+        if not sel and t0 is not None:
+            # a timed region shorter than the sampler's period: the samples nearest to it
+            sel = [x for x in self.samples if x[0] is not None and t0 - 0.25 <= x[0] <= t1 + 0.25]
+            window = "timed region +- 0.25 s"
         sm = [a for _, a, _ in sel]
         mask = 0
         for _, _, r in sel:
             mask |= r
         reasons = sorted(n for n, bit in self.REASONS.items() if mask & bit)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.sm_max, "reasons": reasons,
-                "samples": len(sm), "source": "nvml" if self._nvml else "nvidia-smi",
+                "samples": len(sm), "window": window, "source": "nvml" if self._nvml else "nvidia-smi",
                 "power_w_median": float(np.median(self.power_w)) if self.power_w else None}
 
 

@@ -86,3 +86,20 @@ def test_window_utilisation_and_tune_summary():
     assert out["best_bsize32_aosoa"]["bsize"] == 32 and out["best_bsize32_aosoa"]["layout"] == "aosoa"
     assert set(out["best_per_sorted_windows"]) == {"False", "True"}
     assert out["best_per_threads_per_track"]["1"]["ms"] < out["best_per_threads_per_track"]["2"]["ms"]
+
+
+def test_clock_record_window():
+    """The bench's clock record: the samples inside the timed region, their
+    median and every throttle reason among them; with none inside (a region
+    shorter than the sampler's period) the samples within 0.25 s of it."""
+    bench = _bench_module()
+    c = bench.ClockSampler(0)
+    c.sm_max = 1965.0
+    c.samples = [(0.90, 1500.0, 0x4), (1.00, 1965.0, 0), (1.01, 1965.0, 0x4), (1.02, 1950.0, 0), (1.60, 1200.0, 0x8)]
+    r = c.stop(0.995, 1.025)
+    assert (r["sm_mhz"], r["samples"], r["reasons"], r["window"]) == (1965.0, 3, ["sw_power_cap"], "timed region")
+    c = bench.ClockSampler(0)
+    c.samples = [(0.90, 1900.0, 0), (1.20, 1965.0, 0x8), (2.00, 1000.0, 0x40)]
+    r = c.stop(1.05, 1.10)
+    assert (r["sm_mhz"], r["samples"], r["reasons"]) == (1932.5, 2, ["hw_slowdown"])
+    assert r["window"] == "timed region +- 0.25 s"
