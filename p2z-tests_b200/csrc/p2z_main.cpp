@@ -5,19 +5,25 @@
 // reference's lines -- including the "formatted" line its tools parse and the
 // validation block -- so the reference's scripts can drive it unchanged.
 //
-// usage: p2z_main SEEDFILE [nevts ntrks bsize nlayer niter [smear [cov_scale]]]
+// usage: p2z_main [SEEDFILE [nevts ntrks bsize nlayer niter [smear [cov_scale]]]]
 // SEEDFILE: first line 6 track parameters, 21 covariance elements and the
 // charge; then one line per layer with 3 hit positions and 6 covariance
-// elements (layer order).  The environment variable P2Z_FLAGS (an integer,
+// elements (layer order).  Without arguments -- as the reference's tools run
+// its executables, whose seed is compiled in (tools/compare.sh) -- the seed
+// file is $P2Z_SEED_FILE, else the reference's known-answer seed in the
+// repository beside this executable (../tests/golden/kat_seed.txt), with the
+// reference's default sizes.  The environment variable P2Z_FLAGS (an integer,
 // decimal or 0x-hex) sets p2z_config.flags, e.g. P2Z_FLAGS=0x20 for the
 // reference's own rounding (P2Z_FLAG_REFERENCE_ROUNDING); P2Z_UPDATE selects the
 // update kind (p2z_update_kind, default 0 = KalmanUpdate_v2).
 #include <sys/time.h>
+#include <unistd.h>
 
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "p2z.h"
@@ -28,11 +34,25 @@ static long now_ms() {
   return (long)tv.tv_sec * 1000 + (long)tv.tv_usec / 1000;
 }
 
+// The seed file when none is given: $P2Z_SEED_FILE, else the known-answer
+// seed of the repository this executable was built in.
+static std::string default_seed_file() {
+  if (const char *e = std::getenv("P2Z_SEED_FILE")) return e;
+  char exe[4096];
+  const ssize_t n = readlink("/proc/self/exe", exe, sizeof exe - 1);
+  if (n <= 0) return "tests/golden/kat_seed.txt";
+  exe[n] = 0;
+  std::string dir(exe);
+  dir = dir.substr(0, dir.find_last_of('/'));
+  return dir + "/../tests/golden/kat_seed.txt";
+}
+
 int main(int argc, char **argv) {
-  if (argc < 2) {
-    std::fprintf(stderr, "usage: %s SEEDFILE [nevts ntrks bsize nlayer niter [smear [cov_scale]]]\n", argv[0]);
+  if (argc > 1 && (std::string(argv[1]) == "-h" || std::string(argv[1]) == "--help")) {
+    std::fprintf(stderr, "usage: %s [SEEDFILE [nevts ntrks bsize nlayer niter [smear [cov_scale]]]]\n", argv[0]);
     return 2;
   }
+  const std::string seed_file = argc > 1 ? std::string(argv[1]) : default_seed_file();
   long nevts = argc > 2 ? std::atol(argv[2]) : 100;
   long ntrks = argc > 3 ? std::atol(argv[3]) : 9600;
   int bsize = argc > 4 ? std::atoi(argv[4]) : 32;
@@ -41,9 +61,9 @@ int main(int argc, char **argv) {
   double smear = argc > 7 ? std::atof(argv[7]) : 1e-7;
   double cov_scale = argc > 8 ? std::atof(argv[8]) : 100.0;
 
-  FILE *f = std::fopen(argv[1], "r");
+  FILE *f = std::fopen(seed_file.c_str(), "r");
   if (!f) {
-    std::fprintf(stderr, "cannot open %s\n", argv[1]);
+    std::fprintf(stderr, "cannot open %s\n", seed_file.c_str());
     return 2;
   }
   p2z_atrk trk;

@@ -706,6 +706,29 @@ def test_driver_reproduces_the_reference_printout(p2z):
         assert abs(float(vals[k]) - float(want)) <= 1.5e-6, (k, vals[k], want)
 
 
+def test_driver_runs_as_the_reference_tools_run_it(p2z, tmp_path):
+    """tools/compare.sh runs each executable with no arguments from another
+    directory and keeps the "formatted" line without its first word: the
+    driver then reads the known-answer seed beside its repository, runs the
+    reference's default sizes (100 x 9600, bsize 32, 20 layers, 5 passes) and
+    prints a line of the fields tools/compare.py reads (iterations, events,
+    tracks, bsize, nb, then times)."""
+    import os
+    import subprocess
+    exe = ROOT / "p2z-tests_b200" / "p2z_main"
+    env = {k: v for k, v in os.environ.items() if k != "P2Z_SEED_FILE"}
+    r = subprocess.run(f"{exe} | grep formatted | cut -d' ' -f2-", shell=True, cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr
+    f = r.stdout.split()
+    assert f[:5] == ["5", "100", "9600", "32", "300"], r.stdout
+    assert all(float(x) >= 0 for x in f[5:])
+    # a seed file named by the environment
+    r = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True, text=True, timeout=600,
+                       env=dict(env, P2Z_SEED_FILE=str(tmp_path / "absent.txt")))
+    assert r.returncode == 2 and "absent.txt" in r.stderr
+
+
 @pytest.mark.parametrize("masked", [False, True])
 def test_small_launch_l2_prefetch_same_bits(p2z, ctx, masked):
     """Launches of at most 4 warps per SM first ask L2 for their hit blocks;
