@@ -77,7 +77,8 @@ struct RunArgs {
   int64_t slot_begin, slot_end;    // slots [begin, end) of this launch
   int nlayer;
   float kfact;
-  unsigned int *status;            // bit 0: a det <= 0 was met; bit 1: a staging wait timed out
+  unsigned int *status;            // bit 0: a det <= 0 was met; bit 1: a staging wait timed out;
+                                   // bit 2: a non-finite input word (k_check_inputs)
   unsigned long long *queue;       // persistent kernels: next work item
   int64_t ws;                      // SoA layout (B == 0): slots in the arrays = word stride
   // Sorted windows (masked kernels only): the launch's slots are split into windows
