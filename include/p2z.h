@@ -635,7 +635,8 @@ typedef struct p2z_server_config {
   int32_t bsize;               /* AOSOA width of the submitted events */
   int32_t nlayer;
   int32_t update;              /* p2z_update_kind */
-  uint32_t flags;              /* P2Z_FLAG_ACCURATE_TRIG / REFERENCE_ROUNDING / FULL_HITS */
+  uint32_t flags;              /* P2Z_FLAG_ACCURATE_TRIG / REFERENCE_ROUNDING / FULL_HITS; any other
+                                  flag: p2z_server_create returns P2Z_UNSUPPORTED */
   float kfact;                 /* 0 -> P2Z_KFACT_DEFAULT */
   int64_t device_budget_bytes; /* size of the slot ring */
   int32_t max_inflight;        /* launch groups on the GPU at once; 0 -> 2 */

@@ -328,6 +328,10 @@ p2z_status p2z_server_create(int device, const p2z_server_config *cfg, p2z_serve
   if (cfg->nlayer < 1 || cfg->nlayer > 32 || cfg->update < 0 || cfg->update > P2Z_UPDATE_F64) return P2Z_BAD_ARG;
   if (cfg->device_budget_bytes <= 0) return P2Z_BAD_ARG;
   if ((cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING) && cfg->update != P2Z_UPDATE_V2) return P2Z_UNSUPPORTED;
+  // the flags a group launch honours; the others (STRICT, CHECK_INPUTS, the schedule flags) have no
+  // per-request status or launch form here
+  if (cfg->flags & ~(uint32_t)(P2Z_FLAG_ACCURATE_TRIG | P2Z_FLAG_REFERENCE_ROUNDING | P2Z_FLAG_FULL_HITS))
+    return P2Z_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();

@@ -237,3 +237,18 @@ def test_device_call_stream_selection(p2z):
     assert p2z._stream(None, np.zeros(4, np.float32), 12345, None) is None
     import torch
     assert p2z._stream(None, torch.zeros(4)) is None  # a CPU tensor
+
+
+def test_server_refuses_flags_it_cannot_honour(p2z):
+    """The server's group launches honour the accurate-trigonometry,
+    reference-rounding and full-hit flags only; strict mode and the input
+    scan (no per-request status) and the schedule flags are refused before
+    any device is touched."""
+    for fl in (p2z.FLAG_STRICT, p2z.FLAG_CHECK_INPUTS, p2z.FLAG_SORT_WINDOWS, p2z.FLAG_NO_GRAPH,
+               p2z.FLAG_PER_EVENT_STREAMS):
+        with pytest.raises(p2z.P2zError) as e:
+            p2z.Server(bsize=32, nlayer=20, flags=fl | p2z.FLAG_ACCURATE_TRIG)
+        assert e.value.status == p2z.UNSUPPORTED, fl
+    with pytest.raises(p2z.P2zError) as e:
+        p2z.Server(bsize=32, nlayer=20, update="3x3_f64", flags=p2z.FLAG_REFERENCE_ROUNDING)
+    assert e.value.status == p2z.UNSUPPORTED
