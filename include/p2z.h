@@ -206,7 +206,7 @@ typedef struct p2z_config {
   int32_t block_threads; /* threads per CTA, a multiple of 32 in 32..256; 0 -> the value
                             p2z_autotune measured best on this context for the same update,
                             flags, bsize, layout and masking, else 128 */
-  uint32_t flags;        /* P2Z_FLAG_* */
+  uint32_t flags;        /* P2Z_FLAG_*; any other bit is P2Z_BAD_ARG */
   int32_t layout;        /* p2z_layout of the track, hit and output arrays */
   /* Uneven form (optional, host memory): nevts track counts.  NULL -> uniform. */
   const int64_t *event_ntrks;

@@ -180,6 +180,10 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
   pl.kfact = cfg->kfact != 0.f ? cfg->kfact : (float)(100. / (-0.299792458 * 3.8112));
   pl.upd = cfg->update;
   pl.flags = cfg->flags;
+  constexpr uint32_t kKnownFlags = P2Z_FLAG_CHECK_INPUTS | P2Z_FLAG_STRICT | P2Z_FLAG_NO_GRAPH |
+                                   P2Z_FLAG_ACCURATE_TRIG | P2Z_FLAG_FULL_HITS | P2Z_FLAG_REFERENCE_ROUNDING |
+                                   P2Z_FLAG_PER_EVENT_STREAMS | P2Z_FLAG_SORT_WINDOWS;
+  if (cfg->flags & ~kKnownFlags) return fail(ctx, P2Z_BAD_ARG, "unknown flag bits 0x%x", cfg->flags & ~kKnownFlags);
   if (cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING) {
     if (cfg->update != P2Z_UPDATE_V2)
       return fail(ctx, P2Z_UNSUPPORTED, "P2Z_FLAG_REFERENCE_ROUNDING applies to P2Z_UPDATE_V2 only");

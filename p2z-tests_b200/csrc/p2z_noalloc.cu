@@ -142,6 +142,10 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
     return fail(P2Z_UNSUPPORTED, "P2Z_FLAG_REFERENCE_ROUNDING applies to P2Z_UPDATE_V2 only");
   if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
     return fail(P2Z_BAD_ARG, "block_threads not a multiple of 32 in 32..256");
+  if (cfg->flags & ~(uint32_t)(P2Z_FLAG_CHECK_INPUTS | P2Z_FLAG_STRICT | P2Z_FLAG_NO_GRAPH | P2Z_FLAG_ACCURATE_TRIG |
+                               P2Z_FLAG_FULL_HITS | P2Z_FLAG_REFERENCE_ROUNDING | P2Z_FLAG_PER_EVENT_STREAMS |
+                               P2Z_FLAG_SORT_WINDOWS))
+    return fail(P2Z_BAD_ARG, "unknown flag bits");
   // The status word lives in the shared scratch and no call returns it, so
   // the flags that report through it are refused rather than ignored.
   if (cfg->flags & (P2Z_FLAG_STRICT | P2Z_FLAG_CHECK_INPUTS))

@@ -252,3 +252,19 @@ def test_server_refuses_flags_it_cannot_honour(p2z):
     with pytest.raises(p2z.P2zError) as e:
         p2z.Server(bsize=32, nlayer=20, update="3x3_f64", flags=p2z.FLAG_REFERENCE_ROUNDING)
     assert e.value.status == p2z.UNSUPPORTED
+
+
+def test_unknown_flag_bits_are_refused(p2z):
+    """A config with a flag bit no P2Z_FLAG_* defines is refused (P2Z_BAD_ARG)
+    rather than run with the bit ignored: by the config checks every entry
+    point shares (here through p2z_num_batches) and by the allocation-free
+    entry point."""
+    cfg = p2z.make_config(bsize=32, nevts=1, ntrks=64, nlayer=20, flags=0x100)
+    assert p2z.lib.p2z_num_batches(p2z.C.byref(cfg)) == -1
+    assert "unknown flag bits" in p2z.lib.p2z_last_error(None).decode()
+    cfg.flags = p2z.FLAG_ACCURATE_TRIG
+    assert p2z.lib.p2z_num_batches(p2z.C.byref(cfg)) == 2
+    cfg.flags = 0x80000000
+    rc = p2z.lib.p2z_run_device_noalloc(p2z.C.byref(cfg), None, None, None, None, None)
+    assert rc == p2z.BAD_ARG
+    assert "unknown flag bits" in p2z.lib.p2z_last_error(None).decode()
