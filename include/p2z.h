@@ -198,8 +198,9 @@ typedef struct p2z_config {
                             when event_ntrks is given */
   int32_t nlayer;        /* layers, 1..32 (reference macro nlayer, :35-37) */
   int32_t niter;         /* passes over the whole input (reference NITER, :31-33); each pass
-                            recomputes the outputs from the inputs; 0 is treated as 1 */
-  float kfact;           /* 0 -> P2Z_KFACT_DEFAULT */
+                            recomputes the outputs from the inputs; 0 is treated as 1,
+                            negative is P2Z_BAD_ARG */
+  float kfact;           /* 0 -> P2Z_KFACT_DEFAULT; not finite -> P2Z_BAD_ARG */
   int32_t update;        /* p2z_update_kind */
   int32_t schedule;      /* p2z_schedule; AUTO -> the schedule p2z_autotune measured best on
                             this context for the same key, else the rule under p2z_schedule */

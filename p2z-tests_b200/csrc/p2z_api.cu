@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -173,6 +174,8 @@ p2z_status make_plan(p2z_context *ctx, const p2z_config *cfg, Plan &pl) {
     return fail(ctx, P2Z_BAD_ARG, "block_threads %d not a multiple of 32 in 32..256", cfg->block_threads);
   if (cfg->layout != P2Z_LAYOUT_AOSOA && cfg->layout != P2Z_LAYOUT_SOA)
     return fail(ctx, P2Z_BAD_ARG, "layout %d unknown", cfg->layout);
+  if (cfg->niter < 0) return fail(ctx, P2Z_BAD_ARG, "niter %d < 0", cfg->niter);
+  if (!std::isfinite(cfg->kfact)) return fail(ctx, P2Z_BAD_ARG, "kfact is not finite");
   pl.soa = cfg->layout == P2Z_LAYOUT_SOA;
   pl.B = cfg->bsize;
   pl.nlayer = cfg->nlayer;

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -137,6 +138,8 @@ extern "C" p2z_status p2z_run_device_noalloc(const p2z_config *cfg, const void *
   if (cfg->layout != P2Z_LAYOUT_AOSOA) return fail(P2Z_UNSUPPORTED, "only the AOSOA layout is supported here");
   if (cfg->nlayer < 1 || cfg->nlayer > 32) return fail(P2Z_BAD_ARG, "nlayer not in 1..32");
   if (cfg->nevts < 0) return fail(P2Z_BAD_ARG, "nevts < 0");
+  if (cfg->niter < 0) return fail(P2Z_BAD_ARG, "niter < 0");
+  if (!std::isfinite(cfg->kfact)) return fail(P2Z_BAD_ARG, "kfact is not finite");
   if (cfg->update < P2Z_UPDATE_V2 || cfg->update > P2Z_UPDATE_F64) return fail(P2Z_BAD_ARG, "unknown update kind");
   if ((cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING) && cfg->update != P2Z_UPDATE_V2)
     return fail(P2Z_UNSUPPORTED, "P2Z_FLAG_REFERENCE_ROUNDING applies to P2Z_UPDATE_V2 only");

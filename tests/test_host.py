@@ -268,3 +268,15 @@ def test_unknown_flag_bits_are_refused(p2z):
     rc = p2z.lib.p2z_run_device_noalloc(p2z.C.byref(cfg), None, None, None, None, None)
     assert rc == p2z.BAD_ARG
     assert "unknown flag bits" in p2z.lib.p2z_last_error(None).decode()
+
+
+def test_niter_and_kfact_are_checked(p2z):
+    cfg = p2z.make_config(bsize=32, nevts=1, ntrks=64, nlayer=20, niter=-1)
+    assert p2z.lib.p2z_num_batches(p2z.C.byref(cfg)) == -1
+    cfg.niter = 0
+    assert p2z.lib.p2z_num_batches(p2z.C.byref(cfg)) == 2
+    for k in (float("nan"), float("inf")):
+        cfg.kfact = k
+        assert p2z.lib.p2z_num_batches(p2z.C.byref(cfg)) == -1
+        assert "kfact" in p2z.lib.p2z_last_error(None).decode()
+        assert p2z.lib.p2z_run_device_noalloc(p2z.C.byref(cfg), None, None, None, None, None) == p2z.BAD_ARG
