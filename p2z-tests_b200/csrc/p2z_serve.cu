@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -326,7 +327,9 @@ p2z_status p2z_server_create(int device, const p2z_server_config *cfg, p2z_serve
   if (cfg->abi_version != P2Z_ABI_VERSION) return P2Z_BAD_ARG;
   if (!(cfg->bsize == 8 || cfg->bsize == 16 || cfg->bsize == 32 || cfg->bsize == 64)) return P2Z_UNSUPPORTED;
   if (cfg->nlayer < 1 || cfg->nlayer > 32 || cfg->update < 0 || cfg->update > P2Z_UPDATE_F64) return P2Z_BAD_ARG;
-  if (cfg->device_budget_bytes <= 0) return P2Z_BAD_ARG;
+  if (cfg->device_budget_bytes <= 0 || !std::isfinite(cfg->kfact)) return P2Z_BAD_ARG;
+  if (cfg->block_threads != 0 && (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32))
+    return P2Z_BAD_ARG;
   if ((cfg->flags & P2Z_FLAG_REFERENCE_ROUNDING) && cfg->update != P2Z_UPDATE_V2) return P2Z_UNSUPPORTED;
   // the flags a group launch honours; the others (STRICT, CHECK_INPUTS, the schedule flags) have no
   // per-request status or launch form here

@@ -252,6 +252,10 @@ def test_server_refuses_flags_it_cannot_honour(p2z):
     with pytest.raises(p2z.P2zError) as e:
         p2z.Server(bsize=32, nlayer=20, update="3x3_f64", flags=p2z.FLAG_REFERENCE_ROUNDING)
     assert e.value.status == p2z.UNSUPPORTED
+    for kw in (dict(kfact=float("nan")), dict(block_threads=48), dict(block_threads=512)):
+        with pytest.raises(p2z.P2zError) as e:
+            p2z.Server(bsize=32, nlayer=20, **kw)
+        assert e.value.status == p2z.BAD_ARG, kw
 
 
 def test_unknown_flag_bits_are_refused(p2z):
