@@ -80,6 +80,9 @@ struct p2z_context {
   unsigned int *h_status = nullptr;         // page-locked copy of it (p2z_run)
   unsigned long long *d_queue = nullptr;    // 2 persistent work counters (one per copy stream)
   DevBuf trk, hits, out, mask, valid;       // p2z_run buffers / internal masks
+  // what `mask` holds as an internal padding mask: (mask address, bsize, nlayer, the events' track
+  // counts); empty when it holds anything else (a caller's mask copied by p2z_run)
+  std::vector<int64_t> mask_key;
   DevBuf aux;                               // scratch of the validation reduction
   DevBuf perm;                              // sorted-window permutation (masked runs)
   bool has_graph = false;
@@ -521,21 +524,26 @@ std::vector<uint8_t> batch_valid(const Plan &pl) {
 
 // Builds the padding mask of uneven events into ctx->valid / ctx->mask.
 p2z_status internal_mask(p2z_context *ctx, const Plan &pl, cudaStream_t st, const uint32_t **out) {
+  p2z_status r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots);
+  if (r != P2Z_OK) return r;
+  *out = (const uint32_t *)ctx->mask.p;
+  if (pl.nslots == 0) return P2Z_OK;
+  // the mask depends on the batch width, the layers and the events' track counts only: a call with
+  // the same ones as the last build reuses it (calls on one context are ordered, see p2z.h)
+  const int64_t nev = (int64_t)pl.ev_slot_begin.size() - 1;
+  std::vector<int64_t> key = {(int64_t)(uintptr_t)ctx->mask.p, pl.B, pl.nlayer};
+  key.insert(key.end(), pl.event_ntrks, pl.event_ntrks + nev);
+  if (key == ctx->mask_key) return P2Z_OK;
+  ctx->mask_key.clear();
   const std::vector<uint8_t> valid = batch_valid(pl);
-  p2z_status r = ensure(ctx, ctx->valid, valid.size());
+  r = ensure(ctx, ctx->valid, valid.size());
   if (r != P2Z_OK) return r;
-  r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots);
-  if (r != P2Z_OK) return r;
-  if (pl.nslots == 0) {
-    *out = (const uint32_t *)ctx->mask.p;
-    return P2Z_OK;
-  }
   // (pageable source: the copy is staged before the call returns)
   P2Z_CUDA(ctx, cudaMemcpyAsync(ctx->valid.p, valid.data(), valid.size(), cudaMemcpyHostToDevice, st));
   k_fill_mask<<<(unsigned)((pl.nslots + 255) / 256), 256, 0, st>>>((uint32_t *)ctx->mask.p, (const uint8_t *)ctx->valid.p,
                                                                    pl.nslots, pl.B, all_layers(pl.nlayer));
   P2Z_CUDA(ctx, cudaGetLastError());
-  *out = (const uint32_t *)ctx->mask.p;
+  ctx->mask_key = std::move(key);
   return P2Z_OK;
 }
 
@@ -838,6 +846,7 @@ p2z_status p2z_run(p2z_context *ctx, const p2z_config *cfg, const void *trk_in, 
   if (user_mask) {
     // ctx->mask is also the internal padding mask; a user mask replaces it.
     if ((r = ensure(ctx, ctx->mask, sizeof(uint32_t) * (size_t)pl.nslots)) != P2Z_OK) return r;
+    ctx->mask_key.clear();
     d_mask = (const uint32_t *)ctx->mask.p;
   }
   cudaStream_t s0 = ctx->copy[0], s1 = ctx->copy[1];

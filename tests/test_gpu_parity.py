@@ -753,3 +753,53 @@ def test_small_launch_l2_prefetch_same_bits(p2z, ctx, masked):
         ctx.run_device(c2, dt[:small], dh[:small], small_out, d_mask=None if dm is None else dm[:small * 32])
         torch.cuda.synchronize()
         assert _bitdiff(big_out[:small].cpu().numpy(), small_out.cpu().numpy()) == 0
+
+
+def test_internal_padding_mask_reuse(p2z):
+    """Uneven runs given track counts and no mask build a padding mask in the
+    context and reuse it while the batch width, layers and counts stay the
+    same: repeated calls, new counts in the same array, a caller's mask copied
+    into the same buffer by p2z_run in between, and a larger run -- each equal
+    bit for bit to the same call on a fresh context."""
+    import torch
+    def sample(counts, seed):
+        cfg = p2z.make_config(bsize=32, nevts=len(counts), event_ntrks=counts, nlayer=20)
+        t, h, m = p2z.generate_physics(cfg, p2z.physics_params(seed=seed), with_mask=True)
+        return cfg, t, h, m
+
+    def fresh(cfg, t, h):
+        with p2z.Context(0) as c:
+            out = torch.empty(t.shape, device="cuda")
+            c.run_device(cfg, torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda(), out)
+            return out.cpu().numpy()
+
+    counts = np.array([50, 0, 777, 31, 1000], dtype=np.int64)
+    with p2z.Context(0) as ctx:
+        cfg, t, h, m = sample(counts, 5)
+        want = fresh(cfg, t, h)
+        dt, dh = torch.from_numpy(t).cuda(), torch.from_numpy(h).cuda()
+        for _ in range(2):
+            out = torch.full(t.shape, float("nan"), device="cuda")
+            ctx.run_device(cfg, dt, dh, out)
+            assert np.array_equal(out.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        # new counts in the same host array (the config points at it): the same batches, other padding
+        cfg._event_ntrks_keep[:] = [64, 0, 770, 32, 1010]
+        assert p2z.num_batches(cfg) == 60
+        want2 = fresh(cfg, t, h)
+        assert not np.array_equal(want2.view(np.uint32), want.view(np.uint32))
+        out = torch.empty(t.shape, device="cuda")
+        ctx.run_device(cfg, dt, dh, out)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want2.view(np.uint32))
+        # a caller's mask through p2z_run (copied into the same context buffer), then the padding mask again
+        mm = m.copy()
+        p2z.mask_layers(mm, 20, min_hits=5, max_hits=15, drop_prob=0.2, seed=9)
+        ho = np.empty_like(t)
+        ctx.run(cfg, t, h, ho, hit_mask=mm)
+        out = torch.empty(t.shape, device="cuda")
+        ctx.run_device(cfg, dt, dh, out)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want2.view(np.uint32))
+        # a larger run: a new buffer
+        cfg3, t3, h3, _ = sample(np.array([3000, 5, 4000], dtype=np.int64), 6)
+        out = torch.empty(t3.shape, device="cuda")
+        ctx.run_device(cfg3, torch.from_numpy(t3).cuda(), torch.from_numpy(h3).cuda(), out)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), fresh(cfg3, t3, h3).view(np.uint32))
